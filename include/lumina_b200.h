@@ -1,0 +1,196 @@
+/* lumina_b200.h -- C ABI of the B200 (sm_100a) coupled-dipole solve library.
+ *
+ * This is the drop-in boundary for the reference's compute backend
+ * (crates/lumina-compute/src/backend.rs) and the two solver hooks its
+ * on-the-fly path lacks.  Plain pointers and sizes only; every function
+ * returns a lum_status and never aborts across the ABI.
+ *
+ * Conventions
+ *  - complex arrays are interleaved (re, im) doubles, the memory layout of
+ *    ndarray's Array1<Complex64> / Array2<Complex64> (row-major);
+ *  - a vector of the CDA system has 3N complex entries, entry 3*i+c holding
+ *    component c of dipole i (assembly.rs:178-194);
+ *  - positions are N*3 doubles in nm; alpha^-1 / alpha blocks are N*9
+ *    complex, row-major 3x3 per dipole (types.rs:12-18);
+ *  - "_device" variants take device pointers and an optional cudaStream_t
+ *    (passed as void*; NULL = the session's stream).
+ */
+#ifndef LUMINA_B200_H
+#define LUMINA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define LUM_API __attribute__((visibility("default")))
+#else
+#define LUM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  Map onto ComputeError (backend.rs:13-22) and SolverError
+ * (solver/mod.rs:18-30):
+ *   UNAVAILABLE -> ComputeError::Unavailable, DEVICE -> DeviceError,
+ *   OOM -> OutOfMemory, NOT_CONVERGED -> SolverError::ConvergenceFailure,
+ *   INVALID -> SolverError::InvalidGeometry / LinAlgError. */
+typedef enum {
+  LUM_OK = 0,
+  LUM_ERR_UNAVAILABLE = 1,
+  LUM_ERR_DEVICE = 2,
+  LUM_ERR_OOM = 3,
+  LUM_ERR_NOT_CONVERGED = 4,
+  LUM_ERR_TIMEOUT = 5,
+  LUM_ERR_INVALID = 6
+} lum_status;
+
+/* Arithmetic of a matvec / matrix storage. */
+enum { LUM_FP64 = 0, LUM_FP32 = 1 };
+
+/* Solve modes of lum_solve_gmres. */
+enum {
+  LUM_SOLVE_FP64 = 0,        /* plain FP64 GMRES(m): Arnoldi and matvecs in FP64 */
+  LUM_SOLVE_FP32_REFINE = 1  /* FP32 matvecs inside FP64 Arnoldi/Givens, every
+                                restart residual r = b - A x in FP64 */
+};
+
+typedef struct lum_ctx lum_ctx;
+typedef struct lum_session lum_session;
+
+/* LatticeSpec (crates/lumina-geometry/src/lattice.rs:29-44). is_2d=0 is a
+ * 1D chain along a1 (a2 ignored).  has_eta=0 selects eta = sqrt(pi/A). */
+typedef struct {
+  double a1[3];
+  double a2[3];
+  int is_2d;
+  int has_eta;
+  double eta;
+  int truncation_real;
+  int truncation_recip;
+} lum_lattice;
+
+/* SubstrateRuntime::Fresnel (solver/substrate.rs:103-107): interface plane
+ * and the scalar reflection factor (quasi-static delta-eps or retarded r). */
+typedef struct {
+  double z_interface;
+  double refl_re;
+  double refl_im;
+} lum_substrate;
+
+typedef struct {
+  int iterations;          /* Arnoldi steps, counted as iterative.rs:129 does */
+  int restarts;            /* restart cycles completed */
+  int matvecs_fp64;        /* FP64 operator applications */
+  int matvecs_fp32;        /* FP32 operator applications */
+  int matvecs_reference;   /* matvecs the reference loop would have issued
+                              (it recomputes the cycle-start residual) */
+  int converged;
+  double rel_residual;     /* final true residual / ||b||, FP64 */
+  double seconds;          /* wall time of the solve */
+} lum_solve_info;
+
+/* ---- context ------------------------------------------------------------ */
+/* Creates a context on CUDA device `device`; fails with UNAVAILABLE when no
+ * sm_100 device exists.  Replaces GpuBackend::new_blocking (gpu.rs:115-290). */
+LUM_API int lum_ctx_create(int device, lum_ctx** out);
+LUM_API int lum_ctx_destroy(lum_ctx* ctx);
+/* ComputeBackend::device_info (backend.rs:64, gpu.rs:493-500). */
+LUM_API int lum_device_info(lum_ctx* ctx, char* name, size_t name_len, size_t* memory_bytes,
+                    int* compute_units);
+/* Message of the last failing call on this thread (never NULL). */
+LUM_API const char* lum_last_error(void);
+/* Kernels this library has launched since load (all threads). */
+LUM_API uint64_t lum_launch_count(void);
+
+/* ---- host-side inputs (types.rs, assembly.rs) ---------------------------- */
+/* compute_diagonal_blocks / invert_3x3 (assembly.rs:325-363): alpha^-1 per
+ * dipole; INVALID when |det| <= 1e-30 (the reference panics there). */
+LUM_API int lum_invert_polarisability(int n_dipoles, const double* alpha, double* inv_alpha);
+/* build_incident_field_vector + IncidentField::at_position
+ * (assembly.rs:178-194, types.rs:60-73). */
+LUM_API int lum_incident_field(int n_dipoles, const double* pos, const double direction[3],
+                       const double polarisation[3], double amplitude, double k,
+                       double* rhs);
+/* OpticalSolver::compute_cross_sections (cda/mod.rs:175-236) from solved
+ * moments: out[0]=C_ext, out[1]=C_abs, out[2]=max(C_ext-C_abs,0). */
+LUM_API int lum_cross_sections(int n_dipoles, const double* pos, const double* inv_alpha,
+                       const double* moments, double k, const double direction[3],
+                       const double polarisation[3], double amplitude, double out[3]);
+
+/* ---- sessions (MatvecSession, backend.rs:47-55) -------------------------- */
+/* ComputeBackend::create_session(n) (backend.rs:70-72, gpu.rs:303-399):
+ * a cached-matrix session of dimension dim=3N, storage LUM_FP32 or LUM_FP64. */
+LUM_API int lum_session_create_cached(lum_ctx* ctx, int dim, int storage_precision,
+                              lum_session** out);
+/* MatvecSession::upload_matrix (backend.rs:51, gpu.rs:410-421). */
+LUM_API int lum_session_upload_matrix(lum_session* s, const double* A);
+/* ComputeBackend::assemble_and_create_session (backend.rs:109-117,
+ * gpu.rs:502-610), widened to the FCD / lattice / substrate terms of
+ * assemble_interaction_matrix (assembly.rs:45-175): the whole 3N x 3N matrix
+ * is built on the device.  inv_alpha = compute_diagonal_blocks output. */
+LUM_API int lum_session_assemble(lum_ctx* ctx, int n_dipoles, const double* pos,
+                         const double* inv_alpha, double k, int use_fcd, double cell_size,
+                         const lum_lattice* lattice, const double k_bloch[3],
+                         const lum_substrate* substrate, int storage_precision,
+                         lum_session** out);
+/* New backend hook (the reference's on-the-fly path bypasses the backend,
+ * cda/mod.rs:329-344 and :375-390): a matrix-free session whose matvec is
+ * matvec_on_the_fly (assembly.rs:209-318).  O(N) device memory. */
+LUM_API int lum_session_create_onthefly(lum_ctx* ctx, int n_dipoles, const double* pos,
+                                const double* inv_alpha, double k, int use_fcd,
+                                double cell_size, const lum_lattice* lattice,
+                                const double k_bloch[3], const lum_substrate* substrate,
+                                lum_session** out);
+/* Re-targets an on-the-fly session to a new wavelength (k, alpha^-1,
+ * substrate factor) keeping the geometry and near-pair list (the runner's
+ * per-wavelength loop, runner.rs:150-183). */
+LUM_API int lum_session_set_wavelength(lum_session* s, double k, const double* inv_alpha,
+                               const lum_substrate* substrate);
+/* MatvecSession::matvec (backend.rs:54, gpu.rs:428-488) on host vectors,
+ * precision LUM_FP64 or LUM_FP32 (FP32 arithmetic, FP64 in/out). */
+LUM_API int lum_session_matvec(lum_session* s, int precision, const double* x, double* y);
+LUM_API int lum_session_matvec_device(lum_session* s, int precision, const void* x_dev, void* y_dev,
+                              void* stream);
+/* Multi-RHS cached matvec Y = A X, X and Y row-major dim x nrhs (device). */
+LUM_API int lum_session_matmul_device(lum_session* s, const void* X_dev, void* Y_dev, int nrhs,
+                              void* stream);
+/* Use the caller's stream for all later work of this session (NULL resets). */
+LUM_API int lum_session_set_stream(lum_session* s, void* stream);
+LUM_API int lum_session_destroy(lum_session* s);
+
+/* ---- solve (iterative.rs:33-206; fills the dense_solve slot,
+ *      backend.rs:123-133) -------------------------------------------------- */
+/* Restarted GMRES(min(restart,3N)) with x0 = 0, modified Gram-Schmidt and
+ * complex Givens rotations, |g| < tol*||b|| inside a cycle and the true
+ * residual at its end, as iterative.rs does.  NOT_CONVERGED carries
+ * info->rel_residual.  Host vectors. */
+LUM_API int lum_solve_gmres(lum_session* s, const double* b, double tol, int max_iter, int restart,
+                    int mode, double* x, lum_solve_info* info);
+LUM_API int lum_solve_gmres_device(lum_session* s, const void* b_dev, void* x_dev, double tol,
+                           int max_iter, int restart, int mode, lum_solve_info* info,
+                           void* stream);
+
+/* ---- measurement --------------------------------------------------------- */
+/* While enabled, every launch of the session's dominant matvec kernel (the
+ * dense pair kernel, or the GEMV of a cached session) is bracketed by CUDA
+ * events on the session stream.  lum_session_profile resets the record;
+ * lum_session_kernel_time synchronises and returns the launches and total
+ * milliseconds recorded for one precision (LUM_FP32 / LUM_FP64). */
+LUM_API int lum_session_profile(lum_session* s, int enable);
+LUM_API int lum_session_kernel_time(lum_session* s, int precision, int* launches,
+                                    double* total_ms);
+/* Dense-pair on-the-fly geometry facts: near pairs (FCD) and split factor. */
+LUM_API int lum_session_stats(lum_session* s, long long* near_pairs, int* ell_width, int* nsplit32,
+                      int* nsplit64);
+/* CUDA-core throughput microbenchmark (FMA chains), the roofline
+ * denominator for the compute-bound on-the-fly kernels: FP32 and FP64
+ * GFLOP/s measured on the context's device. */
+LUM_API int lum_measure_fma_peak(lum_ctx* ctx, double* fp32_gflops, double* fp64_gflops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LUMINA_B200_H */

@@ -1,0 +1,281 @@
+// cached.cu -- the dense 3N x 3N interaction matrix on the device.
+//
+// Assembly (assemble_interaction_matrix, assembly.rs:45-175): one thread per
+// dipole pair (i, j) evaluates the 3x3 block once (the reference's WGSL
+// shader re-evaluated G for each of the 9 entries, matrix_assemble.wgsl:59)
+// and writes row segments 3j..3j+2 of rows 3i..3i+2; consecutive threads
+// take consecutive j, so each warp store is a contiguous run of a row.  The
+// alpha^-1 diagonal is written on the device (no host patch,
+// cf. gpu.rs:585-603), the FCD near pairs are corrected by a second pass
+// over the ELL near list, and a substrate image term and the Ewald sum are
+// included as in the reference.
+//
+// Matvec (MatvecSession::matvec): y = A x is bound by reading A from HBM
+// (8 or 16 bytes per complex entry).  One warp per row streams the row with
+// coalesced 8/16-byte loads, x is read through L1/L2 (3N complex is a few
+// MB at most), products accumulate in FP64 and the warp reduces by shuffle.
+#include "lumina_internal.cuh"
+#include "device_physics.cuh"
+
+namespace lum {
+
+
+template <typename T2> __device__ __forceinline__ T2 mk(double re, double im);
+template <> __device__ __forceinline__ float2 mk<float2>(double re, double im) {
+  return make_float2((float)re, (float)im);
+}
+template <> __device__ __forceinline__ double2 mk<double2>(double re, double im) {
+  return make_double2(re, im);
+}
+
+template <typename T2>
+__global__ void __launch_bounds__(128)
+assemble_pairs(int n, const double4* __restrict__ pos, const double2* __restrict__ inv_alpha,
+               double k, int has_lat, LatticeDev L, const double4* __restrict__ lreal,
+               const double4* __restrict__ lrecip, double kb0, double kb1, double kb2,
+               int has_sub, SubstrateDev sub, T2* __restrict__ A) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long npairs = (long long)n * n;
+  if (idx >= npairs) return;
+  const int i = (int)(idx / n), j = (int)(idx % n);
+  const size_t dim = 3 * (size_t)n;
+  const double4 ri = pos[i], rj = pos[j];
+  const double kb[3] = {kb0, kb1, kb2};
+  double2 blk[9];
+  for (int e = 0; e < 9; ++e) blk[e] = make_double2(0.0, 0.0);
+  if (i == j)
+    for (int e = 0; e < 9; ++e) blk[e] = inv_alpha[(size_t)e * n + i];
+  double2 g[9];
+  if (has_lat) {
+    ewald_tensor(L, lreal, lrecip, ri.x - rj.x, ri.y - rj.y, ri.z - rj.z, kb, k, g);
+    for (int e = 0; e < 9; ++e) {
+      blk[e].x -= g[e].x;
+      blk[e].y -= g[e].y;
+    }
+  } else if (i != j) {
+    greens_point_d(ri.x - rj.x, ri.y - rj.y, ri.z - rj.z, k, g);
+    for (int e = 0; e < 9; ++e) {
+      blk[e].x -= g[e].x;
+      blk[e].y -= g[e].y;
+    }
+  }
+  if (has_sub) {  // assembly.rs:129-156, all (i, j) including i == j
+    double dx = ri.x - rj.x, dy = ri.y - rj.y, dz = ri.z - (2.0 * sub.z_interface - rj.z);
+    if (dx * dx + dy * dy + dz * dz >= 1e-20) {
+      if (has_lat)
+        ewald_tensor(L, lreal, lrecip, dx, dy, dz, kb, k, g);
+      else
+        greens_point_d(dx, dy, dz, k, g);
+      const double2 r = make_double2(sub.refl_re, sub.refl_im);
+      const double2 m[3] = {make_double2(-r.x, -r.y), make_double2(-r.x, -r.y), r};
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+          double2 gg = g[3 * a + b];
+          double tr = m[b].x * gg.x - m[b].y * gg.y, ti = m[b].x * gg.y + m[b].y * gg.x;
+          blk[3 * a + b].x -= tr;
+          blk[3 * a + b].y -= ti;
+        }
+    }
+  }
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b)
+      A[(3 * (size_t)i + a) * dim + 3 * (size_t)j + b] = mk<T2>(blk[3 * a + b].x, blk[3 * a + b].y);
+}
+
+// FCD: A[i][j] -= (G_fcd - G_point) for every near pair.
+template <typename T2>
+__global__ void assemble_fcd(int n, int ell_w, const int* __restrict__ near_j,
+                             const double2* __restrict__ fcd, T2* __restrict__ A) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n * ell_w) return;
+  const int w = idx / n, i = idx % n;
+  const int j = near_j[(size_t)w * n + i];
+  if (j < 0) return;
+  const size_t dim = 3 * (size_t)n;
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) {
+      const double2 c = fcd[((size_t)w * 9 + 3 * a + b) * n + i];
+      T2& e = A[(3 * (size_t)i + a) * dim + 3 * (size_t)j + b];
+      e = mk<T2>((double)e.x - c.x, (double)e.y - c.y);
+    }
+}
+
+// y = A x; one warp per row, 4 independent loads in flight per lane.
+template <typename T2>
+__global__ void __launch_bounds__(256)
+gemv_rows(int dim, const T2* __restrict__ A, const double2* __restrict__ x,
+          double2* __restrict__ y) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= dim) return;
+  const T2* row = A + (size_t)warp * dim;
+  double sr = 0.0, si = 0.0;
+  int c = lane;
+  for (; c + 96 < dim; c += 128) {
+    T2 a0 = row[c], a1 = row[c + 32], a2 = row[c + 64], a3 = row[c + 96];
+    double2 x0 = __ldg(&x[c]), x1 = __ldg(&x[c + 32]), x2 = __ldg(&x[c + 64]), x3 = __ldg(&x[c + 96]);
+    sr += (double)a0.x * x0.x - (double)a0.y * x0.y;
+    si += (double)a0.x * x0.y + (double)a0.y * x0.x;
+    sr += (double)a1.x * x1.x - (double)a1.y * x1.y;
+    si += (double)a1.x * x1.y + (double)a1.y * x1.x;
+    sr += (double)a2.x * x2.x - (double)a2.y * x2.y;
+    si += (double)a2.x * x2.y + (double)a2.y * x2.x;
+    sr += (double)a3.x * x3.x - (double)a3.y * x3.y;
+    si += (double)a3.x * x3.y + (double)a3.y * x3.x;
+  }
+  for (; c < dim; c += 32) {
+    T2 a0 = row[c];
+    double2 x0 = __ldg(&x[c]);
+    sr += (double)a0.x * x0.x - (double)a0.y * x0.y;
+    si += (double)a0.x * x0.y + (double)a0.y * x0.x;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    sr += __shfl_down_sync(0xffffffffu, sr, o);
+    si += __shfl_down_sync(0xffffffffu, si, o);
+  }
+  if (lane == 0) y[warp] = make_double2(sr, si);
+}
+
+// Y = A X for nrhs right-hand sides (X, Y row-major dim x nrhs): one warp
+// per row, A read once and applied to NR vectors held in registers.
+template <typename T2, int NR>
+__global__ void __launch_bounds__(256)
+gemm_rows(int dim, const T2* __restrict__ A, const double2* __restrict__ X, int nrhs, int c0,
+          double2* __restrict__ Y) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= dim) return;
+  const T2* row = A + (size_t)warp * dim;
+  double sr[NR], si[NR];
+#pragma unroll
+  for (int r = 0; r < NR; ++r) sr[r] = si[r] = 0.0;
+  for (int c = lane; c < dim; c += 32) {
+    T2 a = row[c];
+    const double2* xr = X + (size_t)c * nrhs + c0;
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      double2 xv = __ldg(&xr[r]);
+      sr[r] += (double)a.x * xv.x - (double)a.y * xv.y;
+      si[r] += (double)a.x * xv.y + (double)a.y * xv.x;
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < NR; ++r) {
+    for (int o = 16; o > 0; o >>= 1) {
+      sr[r] += __shfl_down_sync(0xffffffffu, sr[r], o);
+      si[r] += __shfl_down_sync(0xffffffffu, si[r], o);
+    }
+    if (lane == 0) Y[(size_t)warp * nrhs + c0 + r] = make_double2(sr[r], si[r]);
+  }
+}
+
+__global__ void narrow_rows(size_t count, const double2* __restrict__ src, float2* __restrict__ dst) {
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < count;
+       q += (size_t)gridDim.x * blockDim.x) {
+    double2 v = src[q];
+    dst[q] = make_float2((float)v.x, (float)v.y);
+  }
+}
+
+lum_status CachedOperator::allocate(int dim_, int precision_) {
+  dim = dim_;
+  precision = precision_;
+  size_t es = (precision == LUM_FP32) ? sizeof(float2) : sizeof(double2);
+  LUM_TRY(A.alloc(es * (size_t)dim * dim));
+  return LUM_OK;
+}
+
+lum_status CachedOperator::upload(const double* host, cudaStream_t st) {
+  const size_t count = (size_t)dim * dim;
+  if (precision == LUM_FP64) {
+    LUM_TRY_CUDA(cudaMemcpyAsync(A.p, host, sizeof(double2) * count, cudaMemcpyHostToDevice, st));
+    LUM_TRY_CUDA(cudaStreamSynchronize(st));
+    return LUM_OK;
+  }
+  // FP32 storage: stream the FP64 host matrix through a staging buffer and
+  // narrow on the device, a bounded number of rows at a time.
+  const size_t rows_per = std::max<size_t>(1, (size_t)(64u << 20) / (sizeof(double2) * dim));
+  DevBuf stage;
+  LUM_TRY(stage.alloc(sizeof(double2) * rows_per * dim));
+  for (size_t r0 = 0; r0 < (size_t)dim; r0 += rows_per) {
+    size_t nr = std::min(rows_per, (size_t)dim - r0);
+    size_t cnt = nr * dim;
+    LUM_TRY_CUDA(cudaMemcpyAsync(stage.p, host + 2 * r0 * dim, sizeof(double2) * cnt,
+                                 cudaMemcpyHostToDevice, st));
+    narrow_rows<<<1024, 256, 0, st>>>(cnt, stage.as<double2>(), A.as<float2>() + r0 * dim);
+    LUM_CHECK_LAUNCH();
+  }
+  LUM_TRY_CUDA(cudaStreamSynchronize(st));
+  return LUM_OK;
+}
+
+lum_status CachedOperator::assemble(const OtfOperator& g, cudaStream_t st) {
+  const int n = g.n;
+  const long long npairs = (long long)n * n;
+  const int threads = 128;
+  const long long blocks = (npairs + threads - 1) / threads;
+  if (blocks > 0x7fffffffLL) {
+    set_error("matrix too large for device assembly");
+    return LUM_ERR_INVALID;
+  }
+  if (precision == LUM_FP32)
+    assemble_pairs<float2><<<(unsigned)blocks, threads, 0, st>>>(
+        n, g.pos64.as<double4>(), g.inv_alpha.as<double2>(), g.k, g.has_lattice, g.latdev,
+        g.lat_real.as<double4>(), g.lat_recip.as<double4>(), g.kbloch[0], g.kbloch[1],
+        g.kbloch[2], g.has_substrate, g.substrate, A.as<float2>());
+  else
+    assemble_pairs<double2><<<(unsigned)blocks, threads, 0, st>>>(
+        n, g.pos64.as<double4>(), g.inv_alpha.as<double2>(), g.k, g.has_lattice, g.latdev,
+        g.lat_real.as<double4>(), g.lat_recip.as<double4>(), g.kbloch[0], g.kbloch[1],
+        g.kbloch[2], g.has_substrate, g.substrate, A.as<double2>());
+  LUM_CHECK_LAUNCH();
+  if (g.ell_w > 0 && !g.has_lattice) {
+    const int total = n * g.ell_w;
+    if (precision == LUM_FP32)
+      assemble_fcd<float2><<<(total + 255) / 256, 256, 0, st>>>(
+          n, g.ell_w, g.near_j.as<int>(), g.fcd64.as<double2>(), A.as<float2>());
+    else
+      assemble_fcd<double2><<<(total + 255) / 256, 256, 0, st>>>(
+          n, g.ell_w, g.near_j.as<int>(), g.fcd64.as<double2>(), A.as<double2>());
+    LUM_CHECK_LAUNCH();
+  }
+  return LUM_OK;
+}
+
+lum_status CachedOperator::apply(const double2* x, double2* y, cudaStream_t st) {
+  const int blocks = (int)(((size_t)dim * 32 + 255) / 256);
+  if (precision == LUM_FP32)
+    gemv_rows<float2><<<blocks, 256, 0, st>>>(dim, A.as<float2>(), x, y);
+  else
+    gemv_rows<double2><<<blocks, 256, 0, st>>>(dim, A.as<double2>(), x, y);
+  LUM_CHECK_LAUNCH();
+  return LUM_OK;
+}
+
+lum_status CachedOperator::apply_multi(const double2* X, double2* Y, int nrhs, cudaStream_t st) {
+  const int blocks = (int)(((size_t)dim * 32 + 255) / 256);
+  int c0 = 0;
+  while (c0 < nrhs) {
+    int left = nrhs - c0;
+    int nr = left >= 8 ? 8 : (left >= 4 ? 4 : (left >= 2 ? 2 : 1));
+#define LUM_GEMM_CASE(NRV)                                                                  \
+  case NRV:                                                                                 \
+    if (precision == LUM_FP32)                                                              \
+      gemm_rows<float2, NRV><<<blocks, 256, 0, st>>>(dim, A.as<float2>(), X, nrhs, c0, Y);  \
+    else                                                                                    \
+      gemm_rows<double2, NRV><<<blocks, 256, 0, st>>>(dim, A.as<double2>(), X, nrhs, c0, Y); \
+    break;
+    switch (nr) {
+      LUM_GEMM_CASE(8)
+      LUM_GEMM_CASE(4)
+      LUM_GEMM_CASE(2)
+      LUM_GEMM_CASE(1)
+    }
+#undef LUM_GEMM_CASE
+    LUM_CHECK_LAUNCH();
+    c0 += nr;
+  }
+  return LUM_OK;
+}
+
+}  // namespace lum

@@ -1,0 +1,600 @@
+// capi.cu -- extern "C" surface of liblumina_b200 (declared in
+// include/lumina_b200.h).  Every entry point validates its arguments,
+// converts CUDA failures into lum_status codes with a thread-local message
+// (lum_last_error) and never throws or aborts across the ABI.
+#include "lumina_internal.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdarg>
+#include <cstring>
+#include <new>
+
+namespace lum {
+
+std::atomic<uint64_t> g_launches{0};
+static thread_local std::string t_last_error = "";
+
+void set_error(const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  t_last_error = buf;
+}
+
+lum_status cuda_status(cudaError_t e, const char* what, const char* file, int line) {
+  set_error("%s failed: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();  // clear the sticky-free allocation error
+    return LUM_ERR_OOM;
+  }
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return LUM_ERR_UNAVAILABLE;
+  return LUM_ERR_DEVICE;
+}
+
+lum_status DevBuf::alloc(size_t nbytes) {
+  release();
+  if (nbytes == 0) return LUM_OK;
+  cudaError_t e = cudaMalloc(&p, nbytes);
+  if (e != cudaSuccess) {
+    p = nullptr;
+    size_t fr = 0, tot = 0;
+    cudaGetLastError();
+    cudaMemGetInfo(&fr, &tot);
+    set_error("Out of memory: requested %zu bytes, available %zu", nbytes, fr);
+    return LUM_ERR_OOM;
+  }
+  bytes = nbytes;
+  return LUM_OK;
+}
+
+// --- FMA-chain microbenchmark (roofline denominator for CUDA-core kernels) --
+template <typename T>
+__global__ void fma_chain(T* out, int iters, T a, T b) {
+  T x0 = (T)threadIdx.x * (T)1e-7, x1 = x0 + (T)1, x2 = x0 + (T)2, x3 = x0 + (T)3;
+  T x4 = x0 + (T)4, x5 = x0 + (T)5, x6 = x0 + (T)6, x7 = x0 + (T)7;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      x0 = x0 * a + b; x1 = x1 * a + b; x2 = x2 * a + b; x3 = x3 * a + b;
+      x4 = x4 * a + b; x5 = x5 * a + b; x6 = x6 * a + b; x7 = x7 * a + b;
+    }
+  }
+  T s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+  if (s == (T)-12345.678) out[0] = s;  // keeps the chain live; never true
+}
+
+}  // namespace lum
+
+using namespace lum;
+
+lum_status lum_gmres_device(lum_session* s, const double2* b, double2* x, double tol,
+                            int max_iter, int restart, int mode, lum_solve_info* info,
+                            cudaStream_t st);
+
+lum_status lum_session::apply(int precision, const double2* x, double2* y) {
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (profile) {
+    if (ev_used + 1 > ev_pool.size()) {
+      for (int q = 0; q < 64; ++q) {
+        EvRec r;
+        LUM_TRY_CUDA(cudaEventCreate(&r.a));
+        LUM_TRY_CUDA(cudaEventCreate(&r.b));
+        ev_pool.push_back(r);
+      }
+    }
+    EvRec& r = ev_pool[ev_used++];
+    r.precision = precision;
+    e0 = r.a;
+    e1 = r.b;
+  }
+  if (kind == 0) return otf.apply(precision, x, y, stream, e0, e1);
+  // cached session
+  if (precision == LUM_FP64 && cached.precision == LUM_FP32 && otf.inv_alpha.p)
+    return otf.apply(LUM_FP64, x, y, stream, nullptr, nullptr);
+  if (e0) cudaEventRecord(e0, stream);
+  LUM_TRY(cached.apply(x, y, stream));
+  if (e1) cudaEventRecord(e1, stream);
+  return LUM_OK;
+}
+
+static bool bad_ptr(const void* p, const char* what) {
+  if (!p) {
+    set_error("%s must not be NULL", what);
+    return true;
+  }
+  return false;
+}
+
+extern "C" {
+
+const char* lum_last_error(void) { return t_last_error.c_str(); }
+uint64_t lum_launch_count(void) { return g_launches.load(); }
+
+int lum_ctx_create(int device, lum_ctx** out) {
+  if (bad_ptr(out, "out")) return LUM_ERR_INVALID;
+  *out = nullptr;
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    set_error("No CUDA device found (%s)", cudaGetErrorString(e));
+    return LUM_ERR_UNAVAILABLE;
+  }
+  if (device < 0 || device >= count) {
+    set_error("device %d out of range (count %d)", device, count);
+    return LUM_ERR_INVALID;
+  }
+  cudaDeviceProp prop;
+  LUM_TRY_CUDA(cudaGetDeviceProperties(&prop, device));
+  if (prop.major < 10) {
+    set_error("device %d (%s, sm_%d%d) is not an sm_100 part", device, prop.name, prop.major,
+              prop.minor);
+    return LUM_ERR_UNAVAILABLE;
+  }
+  LUM_TRY_CUDA(cudaSetDevice(device));
+  lum_ctx* c = new (std::nothrow) lum_ctx();
+  if (!c) return LUM_ERR_OOM;
+  c->device = device;
+  c->name = prop.name;
+  c->mem_bytes = prop.totalGlobalMem;
+  c->sms = prop.multiProcessorCount;
+  *out = c;
+  return LUM_OK;
+}
+
+int lum_ctx_destroy(lum_ctx* ctx) {
+  delete ctx;
+  return LUM_OK;
+}
+
+int lum_device_info(lum_ctx* ctx, char* name, size_t name_len, size_t* memory_bytes,
+                    int* compute_units) {
+  if (bad_ptr(ctx, "ctx")) return LUM_ERR_INVALID;
+  if (name && name_len) {
+    std::string s = "GPU (" + ctx->name + ")";
+    std::strncpy(name, s.c_str(), name_len - 1);
+    name[name_len - 1] = '\0';
+  }
+  if (memory_bytes) *memory_bytes = ctx->mem_bytes;
+  if (compute_units) *compute_units = ctx->sms;
+  return LUM_OK;
+}
+
+// ---- host helpers ---------------------------------------------------------
+using cd = std::complex<double>;
+
+static bool invert3(const cd m[9], cd o[9]) {  // assembly.rs:335-363
+  cd a = m[0], b = m[1], c = m[2], d = m[3], e = m[4], f = m[5], g = m[6], h = m[7], k = m[8];
+  cd det = a * (e * k - f * h) - b * (d * k - f * g) + c * (d * h - e * g);
+  if (!(std::abs(det) > 1e-30)) return false;
+  cd id = 1.0 / det;
+  o[0] = id * (e * k - f * h);
+  o[1] = id * (c * h - b * k);
+  o[2] = id * (b * f - c * e);
+  o[3] = id * (f * g - d * k);
+  o[4] = id * (a * k - c * g);
+  o[5] = id * (c * d - a * f);
+  o[6] = id * (d * h - e * g);
+  o[7] = id * (b * g - a * h);
+  o[8] = id * (a * e - b * d);
+  return true;
+}
+
+int lum_invert_polarisability(int n, const double* alpha, double* inv_alpha) {
+  if (n < 0 || (n > 0 && (bad_ptr(alpha, "alpha") || bad_ptr(inv_alpha, "inv_alpha"))))
+    return LUM_ERR_INVALID;
+  for (int i = 0; i < n; ++i) {
+    cd m[9], o[9];
+    for (int e = 0; e < 9; ++e) m[e] = cd(alpha[18 * (size_t)i + 2 * e], alpha[18 * (size_t)i + 2 * e + 1]);
+    if (!invert3(m, o)) {
+      set_error("Singular polarisability tensor at dipole %d", i);
+      return LUM_ERR_INVALID;
+    }
+    for (int e = 0; e < 9; ++e) {
+      inv_alpha[18 * (size_t)i + 2 * e] = o[e].real();
+      inv_alpha[18 * (size_t)i + 2 * e + 1] = o[e].imag();
+    }
+  }
+  return LUM_OK;
+}
+
+int lum_incident_field(int n, const double* pos, const double direction[3],
+                       const double polarisation[3], double amplitude, double k, double* rhs) {
+  if (n < 0 || bad_ptr(direction, "direction") || bad_ptr(polarisation, "polarisation"))
+    return LUM_ERR_INVALID;
+  if (n > 0 && (bad_ptr(pos, "pos") || bad_ptr(rhs, "rhs"))) return LUM_ERR_INVALID;
+  for (int i = 0; i < n; ++i) {
+    const double* p = pos + 3 * (size_t)i;
+    double kdotr = k * (direction[0] * p[0] + direction[1] * p[1] + direction[2] * p[2]);
+    double c = std::cos(kdotr), s = std::sin(kdotr);
+    for (int q = 0; q < 3; ++q) {
+      double e0 = amplitude * polarisation[q];
+      rhs[2 * (3 * (size_t)i + q)] = e0 * c;
+      rhs[2 * (3 * (size_t)i + q) + 1] = e0 * s;
+    }
+  }
+  return LUM_OK;
+}
+
+int lum_cross_sections(int n, const double* pos, const double* inv_alpha, const double* moments,
+                       double k, const double direction[3], const double polarisation[3],
+                       double amplitude, double out[3]) {
+  if (n <= 0 || bad_ptr(pos, "pos") || bad_ptr(inv_alpha, "inv_alpha") ||
+      bad_ptr(moments, "moments") || bad_ptr(out, "out") || bad_ptr(direction, "direction") ||
+      bad_ptr(polarisation, "polarisation"))
+    return LUM_ERR_INVALID;
+  const double e0_sq = amplitude * amplitude;
+  double c_ext = 0.0, c_abs = 0.0;
+  const double k3 = k * k * k;
+  for (int i = 0; i < n; ++i) {
+    const double* p = pos + 3 * (size_t)i;
+    double kdotr = k * (direction[0] * p[0] + direction[1] * p[1] + direction[2] * p[2]);
+    cd phase(std::cos(kdotr), std::sin(kdotr));
+    cd m[3];
+    for (int c = 0; c < 3; ++c)
+      m[c] = cd(moments[2 * (3 * (size_t)i + c)], moments[2 * (3 * (size_t)i + c) + 1]);
+    for (int c = 0; c < 3; ++c) {
+      cd e = amplitude * polarisation[c] * phase;
+      c_ext += (std::conj(e) * m[c]).imag();
+    }
+    cd acc = 0.0;
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) {
+        cd ia(inv_alpha[18 * (size_t)i + 2 * (3 * a + b)], inv_alpha[18 * (size_t)i + 2 * (3 * a + b) + 1]);
+        acc += m[a] * std::conj(ia) * std::conj(m[b]);
+      }
+    double psq = std::norm(m[0]) + std::norm(m[1]) + std::norm(m[2]);
+    c_abs += acc.imag() - (2.0 / 3.0) * k3 * psq;
+  }
+  c_ext *= k / e0_sq;
+  c_abs *= k / e0_sq;
+  out[0] = c_ext;
+  out[1] = c_abs;
+  out[2] = std::max(c_ext - c_abs, 0.0);
+  return LUM_OK;
+}
+
+// ---- sessions -------------------------------------------------------------
+static lum_status new_session(lum_ctx* ctx, int kind, int dim, lum_session** out) {
+  lum_session* s = new (std::nothrow) lum_session();
+  if (!s) return LUM_ERR_OOM;
+  s->ctx = ctx;
+  s->kind = kind;
+  s->dim = dim;
+  s->n_dipoles = dim / 3;
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete s;
+    return cuda_status(e, "stream create", __FILE__, __LINE__);
+  }
+  *out = s;
+  return LUM_OK;
+}
+
+int lum_session_destroy(lum_session* s) {
+  if (!s) return LUM_OK;
+  cudaSetDevice(s->ctx->device);
+  cudaStreamSynchronize(s->stream);
+  for (auto& r : s->ev_pool) {
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+  return LUM_OK;
+}
+
+int lum_session_set_stream(lum_session* s, void* stream) {
+  if (bad_ptr(s, "session")) return LUM_ERR_INVALID;
+  cudaSetDevice(s->ctx->device);
+  cudaStreamSynchronize(s->stream);
+  if (stream) {
+    if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+    s->stream = (cudaStream_t)stream;
+    s->own_stream = false;
+  } else if (!s->own_stream) {
+    LUM_TRY_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    s->own_stream = true;
+  }
+  return LUM_OK;
+}
+
+int lum_session_create_cached(lum_ctx* ctx, int dim, int precision, lum_session** out) {
+  if (bad_ptr(ctx, "ctx") || bad_ptr(out, "out")) return LUM_ERR_INVALID;
+  *out = nullptr;
+  if (dim <= 0 || (precision != LUM_FP32 && precision != LUM_FP64)) {
+    set_error("invalid cached session (dim %d, precision %d)", dim, precision);
+    return LUM_ERR_INVALID;
+  }
+  lum_session* s = nullptr;
+  LUM_TRY(new_session(ctx, 1, dim, &s));
+  lum_status st = s->cached.allocate(dim, precision);
+  if (st != LUM_OK) {
+    lum_session_destroy(s);
+    return st;
+  }
+  *out = s;
+  return LUM_OK;
+}
+
+int lum_session_upload_matrix(lum_session* s, const double* A) {
+  if (bad_ptr(s, "session") || bad_ptr(A, "matrix")) return LUM_ERR_INVALID;
+  if (s->kind != 1) {
+    set_error("upload_matrix needs a cached session");
+    return LUM_ERR_INVALID;
+  }
+  cudaSetDevice(s->ctx->device);
+  return s->cached.upload(A, s->stream);
+}
+
+static lum_status check_physics(int n, const double* inv_alpha, double k) {
+  if (bad_ptr(inv_alpha, "inv_alpha")) return LUM_ERR_INVALID;
+  if (!(k > 0.0) || !std::isfinite(k)) {
+    set_error("wavenumber must be positive and finite (got %g)", k);
+    return LUM_ERR_INVALID;
+  }
+  for (size_t q = 0; q < 18 * (size_t)n; ++q)
+    if (!std::isfinite(inv_alpha[q])) {
+      set_error("non-finite inverse polarisability at dipole %zu", q / 18);
+      return LUM_ERR_INVALID;
+    }
+  return LUM_OK;
+}
+
+static lum_status check_inputs(int n, const double* pos, const double* inv_alpha, double k) {
+  if (n <= 0) {
+    set_error("No dipoles provided");
+    return LUM_ERR_INVALID;
+  }
+  if (bad_ptr(pos, "pos")) return LUM_ERR_INVALID;
+  return check_physics(n, inv_alpha, k);
+}
+
+int lum_session_create_onthefly(lum_ctx* ctx, int n, const double* pos, const double* inv_alpha,
+                                double k, int use_fcd, double cell, const lum_lattice* lattice,
+                                const double k_bloch[3], const lum_substrate* substrate,
+                                lum_session** out) {
+  if (bad_ptr(ctx, "ctx") || bad_ptr(out, "out")) return LUM_ERR_INVALID;
+  *out = nullptr;
+  LUM_TRY(check_inputs(n, pos, inv_alpha, k));
+  if (n > 100000000) {
+    set_error("too many dipoles (%d)", n);
+    return LUM_ERR_INVALID;
+  }
+  lum_session* s = nullptr;
+  LUM_TRY(new_session(ctx, 0, 3 * n, &s));
+  lum_status st = s->otf.build_geometry(pos, n, s->stream);
+  if (st == LUM_OK)
+    st = s->otf.set_physics(k, inv_alpha, use_fcd, cell, lattice, k_bloch, substrate, s->stream);
+  if (st == LUM_OK) {
+    cudaError_t e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) st = cuda_status(e, "session setup", __FILE__, __LINE__);
+  }
+  if (st != LUM_OK) {
+    lum_session_destroy(s);
+    return st;
+  }
+  *out = s;
+  return LUM_OK;
+}
+
+int lum_session_set_wavelength(lum_session* s, double k, const double* inv_alpha,
+                               const lum_substrate* substrate) {
+  if (bad_ptr(s, "session")) return LUM_ERR_INVALID;
+  if (!s->otf.inv_alpha.p) {
+    set_error("set_wavelength needs a geometry session");
+    return LUM_ERR_INVALID;
+  }
+  LUM_TRY(check_physics(s->n_dipoles, inv_alpha, k));
+  cudaSetDevice(s->ctx->device);
+  LUM_TRY(s->otf.set_physics(k, inv_alpha, s->otf.use_fcd, s->otf.cell, nullptr, nullptr,
+                             substrate, s->stream));
+  if (s->kind == 1) LUM_TRY(s->cached.assemble(s->otf, s->stream));
+  LUM_TRY_CUDA(cudaStreamSynchronize(s->stream));
+  return LUM_OK;
+}
+
+int lum_session_assemble(lum_ctx* ctx, int n, const double* pos, const double* inv_alpha,
+                         double k, int use_fcd, double cell, const lum_lattice* lattice,
+                         const double k_bloch[3], const lum_substrate* substrate, int precision,
+                         lum_session** out) {
+  if (bad_ptr(ctx, "ctx") || bad_ptr(out, "out")) return LUM_ERR_INVALID;
+  *out = nullptr;
+  LUM_TRY(check_inputs(n, pos, inv_alpha, k));
+  if (precision != LUM_FP32 && precision != LUM_FP64) {
+    set_error("invalid storage precision %d", precision);
+    return LUM_ERR_INVALID;
+  }
+  lum_session* s = nullptr;
+  LUM_TRY(new_session(ctx, 1, 3 * n, &s));
+  lum_status st = s->otf.build_geometry(pos, n, s->stream);
+  if (st == LUM_OK)
+    st = s->otf.set_physics(k, inv_alpha, use_fcd, cell, lattice, k_bloch, substrate, s->stream);
+  if (st == LUM_OK) st = s->cached.allocate(3 * n, precision);
+  if (st == LUM_OK) st = s->cached.assemble(s->otf, s->stream);
+  if (st == LUM_OK) {
+    cudaError_t e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) st = cuda_status(e, "assembly", __FILE__, __LINE__);
+  }
+  if (st != LUM_OK) {
+    lum_session_destroy(s);
+    return st;
+  }
+  *out = s;
+  return LUM_OK;
+}
+
+int lum_session_matvec_device(lum_session* s, int precision, const void* x, void* y,
+                              void* stream) {
+  if (bad_ptr(s, "session") || bad_ptr(x, "x") || bad_ptr(y, "y")) return LUM_ERR_INVALID;
+  if (precision != LUM_FP32 && precision != LUM_FP64) {
+    set_error("invalid precision %d", precision);
+    return LUM_ERR_INVALID;
+  }
+  cudaSetDevice(s->ctx->device);
+  cudaStream_t keep = s->stream;
+  if (stream) s->stream = (cudaStream_t)stream;
+  lum_status st = s->apply(precision, (const double2*)x, (double2*)y);
+  s->stream = keep;
+  return st;
+}
+
+int lum_session_matvec(lum_session* s, int precision, const double* x, double* y) {
+  if (bad_ptr(s, "session") || bad_ptr(x, "x") || bad_ptr(y, "y")) return LUM_ERR_INVALID;
+  cudaSetDevice(s->ctx->device);
+  const size_t bytes = sizeof(double2) * (size_t)s->dim;
+  if (!s->xbuf.p) {
+    LUM_TRY(s->xbuf.alloc(bytes));
+    LUM_TRY(s->ybuf.alloc(bytes));
+  }
+  LUM_TRY_CUDA(cudaMemcpyAsync(s->xbuf.p, x, bytes, cudaMemcpyHostToDevice, s->stream));
+  LUM_TRY(s->apply(precision, s->xbuf.as<double2>(), s->ybuf.as<double2>()));
+  LUM_TRY_CUDA(cudaMemcpyAsync(y, s->ybuf.p, bytes, cudaMemcpyDeviceToHost, s->stream));
+  LUM_TRY_CUDA(cudaStreamSynchronize(s->stream));
+  return LUM_OK;
+}
+
+int lum_session_matmul_device(lum_session* s, const void* X, void* Y, int nrhs, void* stream) {
+  if (bad_ptr(s, "session") || bad_ptr(X, "X") || bad_ptr(Y, "Y")) return LUM_ERR_INVALID;
+  if (s->kind != 1 || nrhs <= 0) {
+    set_error("matmul needs a cached session and nrhs > 0");
+    return LUM_ERR_INVALID;
+  }
+  cudaSetDevice(s->ctx->device);
+  return s->cached.apply_multi((const double2*)X, (double2*)Y, nrhs,
+                               stream ? (cudaStream_t)stream : s->stream);
+}
+
+int lum_solve_gmres_device(lum_session* s, const void* b, void* x, double tol, int max_iter,
+                           int restart, int mode, lum_solve_info* info, void* stream) {
+  if (bad_ptr(s, "session") || bad_ptr(b, "b") || bad_ptr(x, "x")) return LUM_ERR_INVALID;
+  if (!(tol > 0.0) || max_iter < 0 || restart < 0 || restart > kMaxRestart ||
+      (mode != LUM_SOLVE_FP64 && mode != LUM_SOLVE_FP32_REFINE)) {
+    set_error("invalid solve arguments (tol %g, max_iter %d, restart %d, mode %d)", tol,
+              max_iter, restart, mode);
+    return LUM_ERR_INVALID;
+  }
+  cudaSetDevice(s->ctx->device);
+  cudaStream_t keep = s->stream;
+  if (stream) s->stream = (cudaStream_t)stream;
+  lum_status st = lum_gmres_device(s, (const double2*)b, (double2*)x, tol, max_iter, restart,
+                                   mode, info, s->stream);
+  s->stream = keep;
+  return st;
+}
+
+int lum_solve_gmres(lum_session* s, const double* b, double tol, int max_iter, int restart,
+                    int mode, double* x, lum_solve_info* info) {
+  if (bad_ptr(s, "session") || bad_ptr(b, "b") || bad_ptr(x, "x")) return LUM_ERR_INVALID;
+  cudaSetDevice(s->ctx->device);
+  const size_t bytes = sizeof(double2) * (size_t)s->dim;
+  if (!s->bbuf.p) LUM_TRY(s->bbuf.alloc(bytes));
+  if (!s->xbuf.p) {
+    LUM_TRY(s->xbuf.alloc(bytes));
+    LUM_TRY(s->ybuf.alloc(bytes));
+  }
+  LUM_TRY_CUDA(cudaMemcpyAsync(s->bbuf.p, b, bytes, cudaMemcpyHostToDevice, s->stream));
+  int st = lum_solve_gmres_device(s, s->bbuf.p, s->xbuf.p, tol, max_iter, restart, mode, info,
+                                  nullptr);
+  if (st == LUM_OK || st == LUM_ERR_NOT_CONVERGED) {
+    LUM_TRY_CUDA(cudaMemcpyAsync(x, s->xbuf.p, bytes, cudaMemcpyDeviceToHost, s->stream));
+    LUM_TRY_CUDA(cudaStreamSynchronize(s->stream));
+  }
+  return st;
+}
+
+int lum_session_profile(lum_session* s, int enable) {
+  if (bad_ptr(s, "session")) return LUM_ERR_INVALID;
+  cudaSetDevice(s->ctx->device);
+  LUM_TRY_CUDA(cudaStreamSynchronize(s->stream));
+  s->profile = enable != 0;
+  s->ev_used = 0;
+  return LUM_OK;
+}
+
+int lum_session_kernel_time(lum_session* s, int precision, int* launches, double* total_ms) {
+  if (bad_ptr(s, "session")) return LUM_ERR_INVALID;
+  cudaSetDevice(s->ctx->device);
+  LUM_TRY_CUDA(cudaStreamSynchronize(s->stream));
+  double tot = 0.0;
+  int cnt = 0;
+  for (size_t q = 0; q < s->ev_used; ++q) {
+    const auto& r = s->ev_pool[q];
+    if (r.precision != precision) continue;
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) {
+      tot += ms;
+      ++cnt;
+    } else {
+      cudaGetLastError();
+    }
+  }
+  if (launches) *launches = cnt;
+  if (total_ms) *total_ms = tot;
+  return LUM_OK;
+}
+
+int lum_session_stats(lum_session* s, long long* near_pairs, int* ell_width, int* nsplit32,
+                      int* nsplit64) {
+  if (bad_ptr(s, "session")) return LUM_ERR_INVALID;
+  cudaSetDevice(s->ctx->device);
+  LUM_TRY_CUDA(cudaStreamSynchronize(s->stream));
+  if (near_pairs) {
+    long long np = 0;
+    if (s->otf.ell_w > 0) {
+      std::vector<int> nj((size_t)s->otf.ell_w * s->otf.n);
+      LUM_TRY_CUDA(cudaMemcpy(nj.data(), s->otf.near_j.p, sizeof(int) * nj.size(),
+                              cudaMemcpyDeviceToHost));
+      for (int v : nj) np += (v >= 0);
+    }
+    *near_pairs = np;
+  }
+  if (ell_width) *ell_width = s->otf.ell_w;
+  if (nsplit32) *nsplit32 = s->otf.nsplit32;
+  if (nsplit64) *nsplit64 = s->otf.nsplit64;
+  return LUM_OK;
+}
+
+int lum_measure_fma_peak(lum_ctx* ctx, double* fp32_gflops, double* fp64_gflops) {
+  if (bad_ptr(ctx, "ctx")) return LUM_ERR_INVALID;
+  LUM_TRY_CUDA(cudaSetDevice(ctx->device));
+  DevBuf out;
+  LUM_TRY(out.alloc(16));
+  cudaEvent_t e0, e1;
+  LUM_TRY_CUDA(cudaEventCreate(&e0));
+  LUM_TRY_CUDA(cudaEventCreate(&e1));
+  const int threads = 256;
+  const int blocks = ctx->sms * 8;
+  auto run = [&](bool dbl, int iters, double* gflops) -> lum_status {
+    for (int rep = 0; rep < 2; ++rep) {
+      cudaEventRecord(e0);
+      if (dbl)
+        fma_chain<double><<<blocks, threads>>>(out.as<double>(), iters, 0.999999, 1e-7);
+      else
+        fma_chain<float><<<blocks, threads>>>(out.as<float>(), iters, 0.999999f, 1e-7f);
+      LUM_CHECK_LAUNCH();
+      cudaEventRecord(e1);
+      LUM_TRY_CUDA(cudaEventSynchronize(e1));
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    double flops = 2.0 * 8 * 16 * (double)iters * threads * blocks;
+    *gflops = flops / (ms * 1e-3) / 1e9;
+    return LUM_OK;
+  };
+  double g32 = 0, g64 = 0;
+  lum_status st = run(false, 4096, &g32);
+  if (st == LUM_OK) st = run(true, 1024, &g64);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (fp32_gflops) *fp32_gflops = g32;
+  if (fp64_gflops) *fp64_gflops = g64;
+  return st;
+}
+
+}  // extern "C"

@@ -1,0 +1,194 @@
+// lumina_internal.cuh -- shared declarations of the sm_100a CDA library.
+//
+// Device data layout (HBM):
+//   * complex vectors (3N entries) are interleaved double2/float2, entry 3*i+c
+//     holds component c of dipole i -- the same order as the reference's
+//     Array1<Complex64> (assembly.rs:178-194);
+//   * dipole positions are stored twice: double4 (x, y, z, 0) for the FP64
+//     kernels, and a centred FP32 hi/lo pair (float4 each) for the FP32
+//     kernels, so an FP32 displacement keeps ~1 ulp of its own magnitude;
+//   * per-dipole 3x3 blocks (alpha^-1) are stored element-major [9][N] so a
+//     warp reading one element of 32 consecutive dipoles is coalesced;
+//   * the FCD near-pair corrections are an ELL table [W][N] of source
+//     indices and [W][9][N] complex tensors (W = max near pairs per dipole).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+#include <atomic>
+
+#include "../../include/lumina_b200.h"
+
+namespace lum {
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr int kMaxRestart = 64;
+
+// --- error plumbing --------------------------------------------------------
+void set_error(const char* fmt, ...);
+lum_status cuda_status(cudaError_t e, const char* what, const char* file, int line);
+extern std::atomic<uint64_t> g_launches;
+
+#define LUM_TRY_CUDA(call)                                                  \
+  do {                                                                      \
+    cudaError_t e_ = (call);                                                \
+    if (e_ != cudaSuccess) return ::lum::cuda_status(e_, #call, __FILE__, __LINE__); \
+  } while (0)
+
+#define LUM_CHECK_LAUNCH()                                                  \
+  do {                                                                      \
+    ::lum::g_launches.fetch_add(1, std::memory_order_relaxed);              \
+    cudaError_t e_ = cudaGetLastError();                                    \
+    if (e_ != cudaSuccess) return ::lum::cuda_status(e_, "kernel launch", __FILE__, __LINE__); \
+  } while (0)
+
+#define LUM_TRY(expr)                 \
+  do {                                \
+    lum_status s_ = (expr);           \
+    if (s_ != LUM_OK) return s_;      \
+  } while (0)
+
+// --- device buffer ---------------------------------------------------------
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  lum_status alloc(size_t nbytes);   // frees the old buffer first; zero-size ok
+  template <typename T> T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+// --- physics configuration on the device ----------------------------------
+struct LatticeDev {
+  int is_2d;
+  double eta;
+  int n_real;          // number of real-space lattice points
+  int n_recip;         // number of reciprocal points (2D) or modes (1D)
+  double area;         // cell measure: area (2D) or |a1| (1D)
+  double a1[3];
+  double e_hat[3];     // 1D chain axis
+  double a1_len;
+  long m_max;          // 1D spectral modes
+};
+
+struct SubstrateDev {
+  double z_interface;
+  double refl_re, refl_im;
+};
+
+// --- on-the-fly operator ----------------------------------------------------
+struct OtfOperator {
+  int n = 0;                // dipoles
+  double k = 0.0;
+  int use_fcd = 0;
+  double cell = 0.0;
+  int has_lattice = 0;
+  int has_substrate = 0;
+  lum_lattice lattice{};
+  double kbloch[3] = {0, 0, 0};
+  SubstrateDev substrate{};
+  LatticeDev latdev{};
+  double center[3] = {0, 0, 0};
+  double extent = 0.0;      // bounding-box diagonal (nm)
+  int fast_trig = 1;        // k*extent within the fast FP32 sincos range
+
+  DevBuf pos64;             // double4[n]
+  DevBuf pos_hi, pos_lo;    // float4[n] (centred)
+  DevBuf img_hi, img_lo;    // float4[n] image positions (substrate), centred
+  DevBuf inv_alpha;         // double2[9][n]
+  int ell_w = 0;            // max near pairs per dipole
+  DevBuf near_j;            // int[ell_w][n], -1 padded
+  DevBuf fcd64;             // double2[ell_w][9][n]
+  DevBuf fcd32;             // float2[ell_w][9][n]
+  DevBuf lat_real;          // double4[n_real] real-space lattice points
+  DevBuf lat_recip;         // double4[n_recip] reciprocal points
+  DevBuf partial;           // scratch: FP32 or FP64 partial sums [nsplit][3n]
+  int nsplit32 = 1, nsplit64 = 1;
+  std::vector<double> host_pos;  // double4 host copy (image positions are built from it)
+
+  lum_status build_geometry(const double* pos_host, int n, cudaStream_t st);
+  lum_status set_physics(double k, const double* inv_alpha_host, int use_fcd, double cell,
+                         const lum_lattice* lat, const double* kb, const lum_substrate* sub,
+                         cudaStream_t st);
+  lum_status apply(int precision, const double2* x, double2* y, cudaStream_t st,
+                   cudaEvent_t ev0, cudaEvent_t ev1);
+};
+
+// --- cached (dense matrix) operator ----------------------------------------
+struct CachedOperator {
+  int dim = 0;              // 3N
+  int precision = LUM_FP32; // storage precision of A
+  DevBuf A;                 // float2 or double2 [dim][dim] row-major
+  DevBuf x32;               // float2[dim] staging for FP32 storage
+  lum_status allocate(int dim, int precision);
+  lum_status upload(const double* host, cudaStream_t st);
+  lum_status assemble(const OtfOperator& geo, cudaStream_t st);
+  lum_status apply(const double2* x, double2* y, cudaStream_t st);
+  lum_status apply_multi(const double2* X, double2* Y, int nrhs, cudaStream_t st);
+};
+
+// --- GMRES workspace --------------------------------------------------------
+struct GmresState {
+  double2 H[(kMaxRestart + 1) * kMaxRestart];
+  double cs[kMaxRestart];
+  double2 sn[kMaxRestart];
+  double2 g[kMaxRestart + 1];
+  double2 y[kMaxRestart];
+  double scal[8];   // 0: last norm, 1: h_{j+1,j}, 2: |g[j+1]|, 3: residual norm
+};
+
+struct GmresWork {
+  int len = 0;      // complex entries (3N)
+  int m = 0;
+  DevBuf V, w, r, tmp, partials, counter, state;
+  GmresState* h_state = nullptr;   // pinned mirror of a few scalars
+  int nblk = 0;
+  lum_status ensure(int len, int m, cudaStream_t st);
+  ~GmresWork();
+};
+
+// vector kernels (gmres.cu)
+lum_status vec_norm(const double2* v, int len, GmresWork& W, int slot, cudaStream_t st);
+lum_status read_scalars(GmresWork& W, cudaStream_t st);
+
+}  // namespace lum
+
+// Session (opaque to callers).
+struct lum_ctx {
+  int device = 0;
+  std::string name;
+  size_t mem_bytes = 0;
+  int sms = 0;
+};
+
+struct lum_session {
+  lum_ctx* ctx = nullptr;
+  int kind = 0;                 // 0 on-the-fly, 1 cached
+  int n_dipoles = 0;
+  int dim = 0;                  // 3N
+  cudaStream_t stream = nullptr;
+  bool own_stream = true;
+  lum::OtfOperator otf;
+  lum::CachedOperator cached;
+  lum::GmresWork gw;
+  lum::DevBuf xbuf, ybuf, bbuf; // host-path staging
+  // profiling of the dominant kernel
+  bool profile = false;
+  struct EvRec {
+    cudaEvent_t a, b;
+    int precision;
+  };
+  std::vector<EvRec> ev_pool;
+  size_t ev_used = 0;
+  lum_status apply(int precision, const double2* x, double2* y);
+};

@@ -1,0 +1,367 @@
+"""TEST INFRASTRUCTURE ONLY -- ctypes wrapper of the CPU FP64 oracle.
+
+The oracle (``cda_oracle.cpp``) is a C++ FP64 restatement of the reference's
+coupled-dipole solve path (greens.rs, assembly.rs, iterative.rs, ewald.rs,
+substrate.rs, types.rs, spline.rs, cda/mod.rs).  It is the checker for the
+CUDA library and the timed host-CPU baseline; the product package never
+imports this module.
+
+Complex arrays are numpy complex128 (interleaved re/im doubles in memory).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from ctypes import POINTER, c_double, c_float, c_int
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liblumina_oracle.so")
+
+_dp = POINTER(c_double)
+_ip = POINTER(c_int)
+
+
+class OrcLattice(ctypes.Structure):
+    _fields_ = [
+        ("a1", c_double * 3),
+        ("a2", c_double * 3),
+        ("is_2d", c_int),
+        ("has_eta", c_int),
+        ("eta", c_double),
+        ("truncation_real", c_int),
+        ("truncation_recip", c_int),
+    ]
+
+
+class OrcSubstrate(ctypes.Structure):
+    _fields_ = [("z_interface", c_double), ("refl_re", c_double), ("refl_im", c_double)]
+
+
+def build() -> str:
+    """Compile the oracle library in place (g++, OpenMP)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def _load():
+    if not os.path.exists(_LIB_PATH):
+        build()
+    lib = ctypes.CDLL(_LIB_PATH)
+    sig = {
+        "orc_greens": (c_int, [_dp, _dp, c_double, _dp]),
+        "orc_greens_filtered": (c_int, [_dp, _dp, c_double, c_double, _dp]),
+        "orc_invert_3x3": (c_int, [_dp, _dp]),
+        "orc_incident_field": (None, [c_int, _dp, _dp, _dp, c_double, c_double, _dp]),
+        "orc_ewald_evaluate": (None, [ctypes.c_void_p, _dp, _dp, c_double, c_int, _dp]),
+        "orc_lattice_eta": (c_double, [ctypes.c_void_p]),
+        "orc_erfc": (c_double, [c_double]),
+        "orc_csqrt_pos_imag": (None, [c_double, c_double, _dp]),
+        "orc_bessel": (c_double, [c_int, c_double]),
+        "orc_bessel_kc": (None, [c_int, c_double, c_double, _dp]),
+        "orc_assemble": (c_int, [c_int, _dp, _dp, c_double, c_int, c_double, ctypes.c_void_p,
+                                 _dp, ctypes.c_void_p, _dp, c_int]),
+        "orc_matvec_onthefly": (c_int, [c_int, _dp, _dp, _dp, c_double, c_int, c_double,
+                                        ctypes.c_void_p, _dp, ctypes.c_void_p, _dp, c_int]),
+        "orc_matvec_onthefly_rows": (c_int, [c_int, _dp, _dp, _dp, c_double, c_int, c_double,
+                                             c_int, c_int, _dp, c_int]),
+        "orc_gmres_dense": (c_int, [c_int, _dp, _dp, c_double, c_int, c_int, _dp, _ip, _ip,
+                                    _dp, c_int]),
+        "orc_gmres_onthefly": (c_int, [c_int, _dp, _dp, _dp, c_double, c_int, c_double,
+                                       ctypes.c_void_p, _dp, ctypes.c_void_p, c_double, c_int,
+                                       _dp, _ip, _ip, _dp, c_int]),
+        "orc_lu_solve": (c_int, [c_int, _dp, _dp, _dp]),
+        "orc_cross_sections": (c_int, [c_int, _dp, _dp, _dp, c_double, _dp, _dp, c_double, _dp]),
+        "orc_rrcm": (None, [c_double, c_double, c_double, c_double, c_double, c_int, _dp]),
+        "orc_ellipsoid_tensor": (None, [c_double, _dp, c_double, c_double, c_double, c_double,
+                                        _dp, _dp]),
+        "orc_fresnel": (None, [c_double, c_double, c_double, c_int, _dp]),
+        "orc_spline_build": (None, [c_int, _dp, _dp, _dp]),
+        "orc_spline_eval": (c_double, [c_int, _dp, _dp, _dp, c_double]),
+        "orc_circular_dichroism": (c_double, [c_int, _dp, _dp, c_double]),
+        "orc_wgsl_assemble_f32": (None, [c_int, _dp, _dp, c_double, POINTER(c_float)]),
+        "orc_wgsl_matvec_f32": (None, [c_int, POINTER(c_float), POINTER(c_float),
+                                       POINTER(c_float)]),
+        "orc_max_threads": (c_int, []),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = _load()
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _vec(a, dtype=np.float64):
+    return np.ascontiguousarray(np.asarray(a, dtype=dtype))
+
+
+def _lat(lattice):
+    if lattice is None:
+        return None
+    s = OrcLattice()
+    s.a1[:] = list(lattice.a1)
+    a2 = lattice.a2 if lattice.a2 is not None else (0.0, 0.0, 0.0)
+    s.a2[:] = list(a2)
+    s.is_2d = 1 if lattice.a2 is not None else 0
+    s.has_eta = 1 if lattice.ewald_eta is not None else 0
+    s.eta = float(lattice.ewald_eta or 0.0)
+    s.truncation_real = int(lattice.truncation_real)
+    s.truncation_recip = int(lattice.truncation_recip)
+    return s
+
+
+def _sub(substrate):
+    if substrate is None:
+        return None
+    r = complex(substrate.delta_eps)
+    return OrcSubstrate(float(substrate.z_interface), r.real, r.imag)
+
+
+def _ref(struct):
+    return ctypes.byref(struct) if struct is not None else None
+
+
+def greens(r1, r2, k):
+    out = np.zeros(9, np.complex128)
+    if lib().orc_greens(_p(_vec(r1)), _p(_vec(r2)), k, _p(out.view(np.float64))) != 0:
+        raise ValueError("Self-interaction: r1 and r2 must not coincide")
+    return out.reshape(3, 3)
+
+
+def greens_filtered(r1, r2, k, cell):
+    out = np.zeros(9, np.complex128)
+    lib().orc_greens_filtered(_p(_vec(r1)), _p(_vec(r2)), k, cell, _p(out.view(np.float64)))
+    return out.reshape(3, 3)
+
+
+def invert_3x3(m):
+    m = np.ascontiguousarray(np.asarray(m, np.complex128).reshape(9))
+    out = np.zeros(9, np.complex128)
+    if lib().orc_invert_3x3(_p(m.view(np.float64)), _p(out.view(np.float64))) != 0:
+        raise ValueError("Singular polarisability tensor")
+    return out.reshape(3, 3)
+
+
+def incident_field(pos, k, direction=(0, 0, 1), polarisation=(1, 0, 0), amplitude=1.0):
+    pos = _vec(pos).reshape(-1, 3)
+    n = pos.shape[0]
+    out = np.zeros(3 * n, np.complex128)
+    lib().orc_incident_field(n, _p(pos), _p(_vec(direction)), _p(_vec(polarisation)),
+                             amplitude, k, _p(out.view(np.float64)))
+    return out
+
+
+def ewald(lattice, r, kb, k, part="full"):
+    s = _lat(lattice)
+    out = np.zeros(9, np.complex128)
+    lib().orc_ewald_evaluate(ctypes.byref(s), _p(_vec(r)), _p(_vec(kb)), k,
+                             {"full": 0, "real": 1, "recip": 2}[part], _p(out.view(np.float64)))
+    return out.reshape(3, 3)
+
+
+def lattice_eta(lattice):
+    return lib().orc_lattice_eta(ctypes.byref(_lat(lattice)))
+
+
+def erfc(x):
+    return lib().orc_erfc(float(x))
+
+
+def csqrt_positive_imag(z):
+    out = np.zeros(2)
+    lib().orc_csqrt_pos_imag(complex(z).real, complex(z).imag, _p(out))
+    return complex(out[0], out[1])
+
+
+_BESSEL = {"j0": 0, "j1": 1, "y0": 2, "y1": 3, "i0": 4, "i1": 5, "k0": 6, "k1": 7}
+
+
+def bessel(name, x):
+    return lib().orc_bessel(_BESSEL[name], float(x))
+
+
+def bessel_kc(order, z):
+    out = np.zeros(2)
+    lib().orc_bessel_kc(order, complex(z).real, complex(z).imag, _p(out))
+    return complex(out[0], out[1])
+
+
+def _alpha_arr(alpha, n):
+    a = np.ascontiguousarray(np.asarray(alpha, np.complex128).reshape(n, 9))
+    return a
+
+
+def assemble(pos, alpha, k, use_fcd=False, cell_size=3.0, lattice=None, k_bloch=(0, 0, 0),
+             substrate=None, nthreads=0):
+    pos = _vec(pos).reshape(-1, 3)
+    n = pos.shape[0]
+    a = _alpha_arr(alpha, n)
+    A = np.zeros((3 * n, 3 * n), np.complex128)
+    ls, ss = _lat(lattice), _sub(substrate)
+    rc = lib().orc_assemble(n, _p(pos), _p(a.view(np.float64)), k, int(use_fcd), cell_size,
+                            _ref(ls), _p(_vec(k_bloch)), _ref(ss), _p(A.view(np.float64)),
+                            nthreads)
+    if rc != 0:
+        raise ValueError("singular polarisability")
+    return A
+
+
+def matvec_onthefly(pos, alpha, x, k, use_fcd=False, cell_size=3.0, lattice=None,
+                    k_bloch=(0, 0, 0), substrate=None, nthreads=0):
+    pos = _vec(pos).reshape(-1, 3)
+    n = pos.shape[0]
+    a = _alpha_arr(alpha, n)
+    x = np.ascontiguousarray(np.asarray(x, np.complex128))
+    y = np.zeros(3 * n, np.complex128)
+    ls, ss = _lat(lattice), _sub(substrate)
+    rc = lib().orc_matvec_onthefly(n, _p(pos), _p(a.view(np.float64)), _p(x.view(np.float64)),
+                                   k, int(use_fcd), cell_size, _ref(ls), _p(_vec(k_bloch)),
+                                   _ref(ss), _p(y.view(np.float64)), nthreads)
+    if rc != 0:
+        raise ValueError("singular polarisability")
+    return y
+
+
+def matvec_onthefly_rows(pos, alpha, x, k, use_fcd, cell_size, row0, row1, nthreads=0):
+    pos = _vec(pos).reshape(-1, 3)
+    n = pos.shape[0]
+    a = _alpha_arr(alpha, n)
+    x = np.ascontiguousarray(np.asarray(x, np.complex128))
+    y = np.zeros(3 * (row1 - row0), np.complex128)
+    lib().orc_matvec_onthefly_rows(n, _p(pos), _p(a.view(np.float64)), _p(x.view(np.float64)),
+                                   k, int(use_fcd), cell_size, row0, row1,
+                                   _p(y.view(np.float64)), nthreads)
+    return y
+
+
+class GmresResult:
+    def __init__(self, x, status, iterations, matvecs, rel_residual):
+        self.x = x
+        self.status = status
+        self.iterations = iterations
+        self.matvecs = matvecs
+        self.rel_residual = rel_residual
+
+    @property
+    def converged(self):
+        return self.status == 0
+
+
+def gmres_dense(A, b, tol, max_iter, restart=30, nthreads=0):
+    A = np.ascontiguousarray(np.asarray(A, np.complex128))
+    b = np.ascontiguousarray(np.asarray(b, np.complex128))
+    n = b.shape[0]
+    x = np.zeros(n, np.complex128)
+    it, mv, rr = c_int(0), c_int(0), c_double(0)
+    st = lib().orc_gmres_dense(n, _p(A.view(np.float64)), _p(b.view(np.float64)), tol, max_iter,
+                               restart, _p(x.view(np.float64)), ctypes.byref(it),
+                               ctypes.byref(mv), ctypes.byref(rr), nthreads)
+    return GmresResult(x, st, it.value, mv.value, rr.value)
+
+
+def gmres_onthefly(pos, alpha, b, k, use_fcd=False, cell_size=3.0, lattice=None,
+                   k_bloch=(0, 0, 0), substrate=None, tol=1e-6, max_iter=1000, nthreads=0):
+    pos = _vec(pos).reshape(-1, 3)
+    n = pos.shape[0]
+    a = _alpha_arr(alpha, n)
+    b = np.ascontiguousarray(np.asarray(b, np.complex128))
+    x = np.zeros(3 * n, np.complex128)
+    it, mv, rr = c_int(0), c_int(0), c_double(0)
+    ls, ss = _lat(lattice), _sub(substrate)
+    st = lib().orc_gmres_onthefly(n, _p(pos), _p(a.view(np.float64)), _p(b.view(np.float64)), k,
+                                  int(use_fcd), cell_size, _ref(ls), _p(_vec(k_bloch)), _ref(ss),
+                                  tol, max_iter, _p(x.view(np.float64)), ctypes.byref(it),
+                                  ctypes.byref(mv), ctypes.byref(rr), nthreads)
+    return GmresResult(x, st, it.value, mv.value, rr.value)
+
+
+def lu_solve(A, b):
+    A = np.ascontiguousarray(np.asarray(A, np.complex128))
+    b = np.ascontiguousarray(np.asarray(b, np.complex128))
+    x = np.zeros_like(b)
+    if lib().orc_lu_solve(b.shape[0], _p(A.view(np.float64)), _p(b.view(np.float64)),
+                          _p(x.view(np.float64))) != 0:
+        raise ValueError("singular matrix")
+    return x
+
+
+def cross_sections(pos, alpha, moments, k, direction=(0, 0, 1), polarisation=(1, 0, 0),
+                   amplitude=1.0):
+    pos = _vec(pos).reshape(-1, 3)
+    n = pos.shape[0]
+    a = _alpha_arr(alpha, n)
+    m = np.ascontiguousarray(np.asarray(moments, np.complex128).reshape(3 * n))
+    out = np.zeros(3)
+    lib().orc_cross_sections(n, _p(pos), _p(a.view(np.float64)), _p(m.view(np.float64)), k,
+                             _p(_vec(direction)), _p(_vec(polarisation)), amplitude, _p(out))
+    return out
+
+
+def rrcm(volume, eps, eps_m, k, radiative=True):
+    out = np.zeros(2)
+    eps = complex(eps)
+    lib().orc_rrcm(volume, eps.real, eps.imag, eps_m, k, int(radiative), _p(out))
+    return complex(out[0], out[1])
+
+
+def ellipsoid_tensor(volume, depol, eps, eps_m, k, rot):
+    out = np.zeros(9, np.complex128)
+    eps = complex(eps)
+    lib().orc_ellipsoid_tensor(volume, _p(_vec(depol)), eps.real, eps.imag, eps_m, k,
+                               _p(_vec(rot)), _p(out.view(np.float64)))
+    return out.reshape(3, 3)
+
+
+def fresnel(eps_sub, eps_env, retarded=True):
+    out = np.zeros(2)
+    e = complex(eps_sub)
+    lib().orc_fresnel(e.real, e.imag, eps_env, int(retarded), _p(out))
+    return complex(out[0], out[1])
+
+
+def spline(xs, ys):
+    xs, ys = _vec(xs), _vec(ys)
+    y2 = np.zeros_like(xs)
+    lib().orc_spline_build(len(xs), _p(xs), _p(ys), _p(y2))
+
+    def ev(x):
+        return lib().orc_spline_eval(len(xs), _p(xs), _p(ys), _p(y2), float(x))
+
+    return ev
+
+
+def circular_dichroism(mom_x, mom_y, k):
+    mx = np.ascontiguousarray(np.asarray(mom_x, np.complex128).reshape(-1))
+    my = np.ascontiguousarray(np.asarray(mom_y, np.complex128).reshape(-1))
+    return lib().orc_circular_dichroism(mx.shape[0] // 3, _p(mx.view(np.float64)),
+                                        _p(my.view(np.float64)), k)
+
+
+def wgsl_assemble_f32(pos, inv_alpha, k):
+    pos = _vec(pos).reshape(-1, 3)
+    n = pos.shape[0]
+    ia = np.ascontiguousarray(np.asarray(inv_alpha, np.complex128).reshape(n, 9))
+    A = np.zeros((3 * n, 3 * n), np.complex64)
+    lib().orc_wgsl_assemble_f32(n, _p(pos), _p(ia.view(np.float64)), k,
+                                A.view(np.float32).ctypes.data_as(POINTER(c_float)))
+    return A
+
+
+def max_threads():
+    return lib().orc_max_threads()
