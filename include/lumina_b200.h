@@ -189,6 +189,23 @@ LUM_API int lum_session_stats(lum_session* s, long long* near_pairs, int* ell_wi
  * GFLOP/s measured on the context's device. */
 LUM_API int lum_measure_fma_peak(lum_ctx* ctx, double* fp32_gflops, double* fp64_gflops);
 
+/* ---- allocation-free matvec ---------------------------------------------- */
+/* No counterpart in the reference.  For callers that cannot let a library
+ * allocate device memory (their HBM is owned by another allocator or reserved
+ * up front, or allocation is not allowed where they call from):
+ * y = alpha^-1 x - sum_{j != i} G(r_i - r_j) x_j, the FP64 point-dipole
+ * on-the-fly matvec (use_fcd = 0), from caller-owned device arrays only --
+ * pos N*3 doubles, inv_alpha N*9 complex, x and y 3N complex -- on `stream`
+ * (NULL = the legacy default stream) of the current device.  Its scratch is a
+ * fixed 8 MiB device array inside the library; N above 174,762 is rejected
+ * with LUM_ERR_INVALID.  The first call on each device looks up that array's
+ * device address, so make it before any stream capture.  All calls share the
+ * array: calls that overlap on the GPU race and must be serialised.  Nothing
+ * is allocated or freed. */
+LUM_API int lum_matvec_onthefly_noalloc(int n_dipoles, const double* pos_dev,
+                                        const double* inv_alpha_dev, double k,
+                                        const double* x_dev, double* y_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -94,6 +94,8 @@ SIGNATURES = {
     "lum_session_stats": (c_int, [c_void_p, POINTER(c_longlong), POINTER(c_int), POINTER(c_int),
                                   POINTER(c_int)]),
     "lum_measure_fma_peak": (c_int, [c_void_p, POINTER(c_double), POINTER(c_double)]),
+    "lum_matvec_onthefly_noalloc": (c_int, [c_int, c_void_p, c_void_p, c_double, c_void_p,
+                                            c_void_p, c_void_p]),
 }
 
 _lib = None
