@@ -184,6 +184,10 @@ LUM_API int lum_session_kernel_time(lum_session* s, int precision, int* launches
 /* Dense-pair on-the-fly geometry facts: near pairs (FCD) and split factor. */
 LUM_API int lum_session_stats(lum_session* s, long long* near_pairs, int* ell_width, int* nsplit32,
                       int* nsplit64);
+/* Kernel configuration chosen for this session (autotuned FP32 pair-kernel
+ * variant, split factors, near-list width, FP32 position mode) as a
+ * "key=value ..." string. */
+LUM_API int lum_session_kernel_config(lum_session* s, char* buf, size_t len);
 /* CUDA-core throughput microbenchmark (FMA chains), the roofline
  * denominator for the compute-bound on-the-fly kernels: FP32 and FP64
  * GFLOP/s measured on the context's device. */

@@ -93,6 +93,7 @@ SIGNATURES = {
     "lum_session_kernel_time": (c_int, [c_void_p, c_int, POINTER(c_int), POINTER(c_double)]),
     "lum_session_stats": (c_int, [c_void_p, POINTER(c_longlong), POINTER(c_int), POINTER(c_int),
                                   POINTER(c_int)]),
+    "lum_session_kernel_config": (c_int, [c_void_p, c_char_p, c_size_t]),
     "lum_measure_fma_peak": (c_int, [c_void_p, POINTER(c_double), POINTER(c_double)]),
     "lum_matvec_onthefly_noalloc": (c_int, [c_int, c_void_p, c_void_p, c_double, c_void_p,
                                             c_void_p, c_void_p]),

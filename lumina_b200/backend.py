@@ -262,6 +262,22 @@ class CudaSession:
         return {"near_pairs": npairs.value, "ell_width": w.value, "nsplit32": s32.value,
                 "nsplit64": s64.value}
 
+    def kernel_config(self) -> dict:
+        """Autotuned kernel choices of this session."""
+        buf = ctypes.create_string_buffer(512)
+        _raise(self._lib.lum_session_kernel_config(self._h, buf, 512), "kernel_config")
+        out = {}
+        for tok in buf.value.decode().split():
+            key, _, val = tok.partition("=")
+            try:
+                out[key] = int(val)
+            except ValueError:
+                try:
+                    out[key] = float(val)
+                except ValueError:
+                    out[key] = val
+        return out
+
     def close(self) -> None:
         if self._h:
             self._lib.lum_session_destroy(self._h)

@@ -104,7 +104,8 @@ __global__ void assemble_fcd(int n, int ell_w, const int* __restrict__ near_j,
 template <typename T2>
 __global__ void __launch_bounds__(256)
 gemv_rows(int dim, const T2* __restrict__ A, const double2* __restrict__ x,
-          double2* __restrict__ y) {
+          double2* __restrict__ y, const int* __restrict__ skip) {
+  if (skip && *skip) return;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= dim) return;
@@ -242,12 +243,13 @@ lum_status CachedOperator::assemble(const OtfOperator& g, cudaStream_t st) {
   return LUM_OK;
 }
 
-lum_status CachedOperator::apply(const double2* x, double2* y, cudaStream_t st) {
+lum_status CachedOperator::apply(const double2* x, double2* y, cudaStream_t st,
+                                 const int* skip) {
   const int blocks = (int)(((size_t)dim * 32 + 255) / 256);
   if (precision == LUM_FP32)
-    gemv_rows<float2><<<blocks, 256, 0, st>>>(dim, A.as<float2>(), x, y);
+    gemv_rows<float2><<<blocks, 256, 0, st>>>(dim, A.as<float2>(), x, y, skip);
   else
-    gemv_rows<double2><<<blocks, 256, 0, st>>>(dim, A.as<double2>(), x, y);
+    gemv_rows<double2><<<blocks, 256, 0, st>>>(dim, A.as<double2>(), x, y, skip);
   LUM_CHECK_LAUNCH();
   return LUM_OK;
 }

@@ -75,7 +75,7 @@ lum_status lum_gmres_device(lum_session* s, const double2* b, double2* x, double
                             int max_iter, int restart, int mode, lum_solve_info* info,
                             cudaStream_t st);
 
-lum_status lum_session::apply(int precision, const double2* x, double2* y) {
+lum_status lum_session::apply(int precision, const double2* x, double2* y, const int* skip) {
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (profile) {
     if (ev_used + 1 > ev_pool.size()) {
@@ -91,12 +91,12 @@ lum_status lum_session::apply(int precision, const double2* x, double2* y) {
     e0 = r.a;
     e1 = r.b;
   }
-  if (kind == 0) return otf.apply(precision, x, y, stream, e0, e1);
+  if (kind == 0) return otf.apply(precision, x, y, stream, e0, e1, skip);
   // cached session
   if (precision == LUM_FP64 && cached.precision == LUM_FP32 && otf.inv_alpha.p)
-    return otf.apply(LUM_FP64, x, y, stream, nullptr, nullptr);
+    return otf.apply(LUM_FP64, x, y, stream, nullptr, nullptr, skip);
   if (e0) cudaEventRecord(e0, stream);
-  LUM_TRY(cached.apply(x, y, stream));
+  LUM_TRY(cached.apply(x, y, stream, skip));
   if (e1) cudaEventRecord(e1, stream);
   return LUM_OK;
 }
@@ -557,6 +557,17 @@ int lum_session_stats(lum_session* s, long long* near_pairs, int* ell_width, int
   if (ell_width) *ell_width = s->otf.ell_w;
   if (nsplit32) *nsplit32 = s->otf.nsplit32;
   if (nsplit64) *nsplit64 = s->otf.nsplit64;
+  return LUM_OK;
+}
+
+int lum_session_kernel_config(lum_session* s, char* buf, size_t len) {
+  if (bad_ptr(s, "session") || bad_ptr(buf, "buf") || len == 0) return LUM_ERR_INVALID;
+  const lum::OtfOperator& o = s->otf;
+  snprintf(buf, len,
+           "kind=%s f32_variant=%s tuned_ms=%.4f nsplit32=%d nsplit64=%d ell_w=%d lofree=%d "
+           "fast_trig=%d",
+           s->kind == 0 ? "onthefly" : "cached", lum::f32_variant_name(o.f32_variant),
+           (double)o.tuned_ms, o.nsplit32, o.nsplit64, o.ell_w, o.lofree, o.fast_trig);
   return LUM_OK;
 }
 

@@ -16,6 +16,7 @@
 
 #include <chrono>
 #include <cmath>
+#include <cstddef>
 
 namespace lum {
 
@@ -54,8 +55,10 @@ __device__ double2 block_sum2(double2 v) {
   return v;
 }
 
-// Publishes this block's partial; returns true in the last block to finish,
-// whose thread 0 then holds the ordered total in *total.
+// Publishes this block's partial; returns true (in every thread) in the last
+// block to finish, whose thread 0 then holds the total in *total.  The last
+// block sums the partials with all its threads and a fixed-shape tree, so
+// the result does not depend on which block finished last.
 __device__ bool last_block_total(double2 part, double2* partials, unsigned* counter,
                                  double2* total) {
   __shared__ bool am_last;
@@ -67,15 +70,16 @@ __device__ bool last_block_total(double2 part, double2* partials, unsigned* coun
   }
   __syncthreads();
   if (!am_last) return false;
+  __threadfence();
+  double2 v = make_double2(0.0, 0.0);
+  for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+    const double2 p = __ldcg(&partials[b]);  // L2: written by other blocks
+    v.x += p.x;
+    v.y += p.y;
+  }
+  v = block_sum2(v);
   if (threadIdx.x == 0) {
-    __threadfence();
-    double2 s = make_double2(0.0, 0.0);
-    volatile double2* vp = partials;
-    for (unsigned b = 0; b < gridDim.x; ++b) {
-      s.x += vp[b].x;
-      s.y += vp[b].y;
-    }
-    *total = s;
+    *total = v;
     *counter = 0u;
   }
   return true;
@@ -124,12 +128,18 @@ k_start_cycle(int len, const double2* __restrict__ r, double2* __restrict__ v0, 
   if (blockIdx.x == 0 && threadIdx.x <= m) {
     S->g[threadIdx.x] = make_double2(threadIdx.x == 0 ? beta : 0.0, 0.0);
   }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    S->done = 0;
+    S->jdone = 0;
+    S->bad = 0;
+  }
 }
 
 // MGS projection i of column j: w -= h_{i-1,j} v_{i-1} (i>0); h_{i,j} = <v_i, w>.
 __global__ void __launch_bounds__(kVecThreads)
 k_mgs(int len, double2* __restrict__ w, const double2* __restrict__ V, int i, int j,
       double2* partials, unsigned* counter, GmresState* S) {
+  if (S->done) return;  // grid-uniform
   const double2* vi = V + (size_t)i * len;
   const double2* vp = V + (size_t)(i > 0 ? i - 1 : 0) * len;
   const double2 hp = (i > 0) ? S->H[(i - 1) * kM + j] : make_double2(0.0, 0.0);
@@ -173,9 +183,15 @@ __device__ void givens(double2 a, double2 b, double* c, double2* s) {
 
 // Last projection of column j, ||w||, then (single thread) the rotations of
 // iterative.rs:98-127.  |g_{j+1}| -> S->scal[2], h_{j+1,j} -> S->scal[1].
+// The step's convergence test runs here too: |g_{j+1}| < abs_tol (the
+// reference's in-cycle test, iterative.rs:133) or, in the refinement mode,
+// below inner_thr; either ends the cycle by setting S->done, which turns the
+// kernels already queued for later steps of the cycle into no-ops.
 __global__ void __launch_bounds__(kVecThreads)
 k_mgs_final(int len, double2* __restrict__ w, const double2* __restrict__ V, int j,
-            double2* partials, unsigned* counter, GmresState* S) {
+            double2* partials, unsigned* counter, GmresState* S, double abs_tol,
+            double inner_thr) {
+  if (S->done) return;  // grid-uniform
   const double2* vj = V + (size_t)j * len;
   const double2 hp = S->H[j * kM + j];
   double2 acc = make_double2(0.0, 0.0);
@@ -189,43 +205,68 @@ k_mgs_final(int len, double2* __restrict__ w, const double2* __restrict__ V, int
   }
   acc = block_sum2(acc);
   double2 tot;
-  if (last_block_total(acc, partials, counter, &tot) && threadIdx.x == 0) {
-    const double hn = sqrt(tot.x);
-    S->scal[1] = hn;
-    double2* H = S->H;
-    H[(j + 1) * kM + j] = make_double2(hn, 0.0);
+  __shared__ double s_hn;
+  __shared__ double2 sH[kM + 1], sS[kM], sG[2];
+  __shared__ double sC[kM];
+  if (!last_block_total(acc, partials, counter, &tot)) return;  // block-uniform
+  // last block: stage column j, the rotations and g[j..j+1] in shared memory
+  const int t = threadIdx.x;
+  if (t == 0) s_hn = sqrt(tot.x);
+  if (t <= j) sH[t] = S->H[t * kM + j];
+  if (t < j) {
+    sC[t] = S->cs[t];
+    sS[t] = S->sn[t];
+  }
+  if (t < 2) sG[t] = S->g[j + t];
+  __syncthreads();
+  if (t == 0) {
+    const double hn = s_hn;
+    sH[j + 1] = make_double2(hn, 0.0);
     for (int i = 0; i < j; ++i) {
-      double c = S->cs[i];
-      double2 s = S->sn[i];
-      double2 hij = H[i * kM + j], hi1 = H[(i + 1) * kM + j];
-      double2 t1 = dmul(s, hi1);
-      double2 temp = make_double2(c * hij.x + t1.x, c * hij.y + t1.y);
-      double2 t2 = dmul(make_double2(-s.x, s.y), hij);  // -conj(s) * h_ij
-      H[(i + 1) * kM + j] = make_double2(t2.x + c * hi1.x, t2.y + c * hi1.y);
-      H[i * kM + j] = temp;
+      const double c = sC[i];
+      const double2 s = sS[i];
+      const double2 hij = sH[i], hi1 = sH[i + 1];
+      const double2 t1 = dmul(s, hi1);
+      const double2 temp = make_double2(c * hij.x + t1.x, c * hij.y + t1.y);
+      const double2 t2 = dmul(make_double2(-s.x, s.y), hij);  // -conj(s) * h_ij
+      sH[i + 1] = make_double2(t2.x + c * hi1.x, t2.y + c * hi1.y);
+      sH[i] = temp;
     }
     double c;
     double2 s;
-    givens(H[j * kM + j], H[(j + 1) * kM + j], &c, &s);
+    givens(sH[j], sH[j + 1], &c, &s);
+    const double2 hjj = sH[j], hj1 = sH[j + 1];
+    const double2 t1 = dmul(s, hj1);
+    sH[j] = make_double2(c * hjj.x + t1.x, c * hjj.y + t1.y);
+    sH[j + 1] = make_double2(0.0, 0.0);
+    const double2 gj = sG[0], gj1 = sG[1];
+    const double2 t3 = dmul(s, gj1);
+    const double2 t4 = dmul(make_double2(-s.x, s.y), gj);
+    const double2 g1 = make_double2(t4.x + c * gj1.x, t4.y + c * gj1.y);
+    S->g[j] = make_double2(c * gj.x + t3.x, c * gj.y + t3.y);
+    S->g[j + 1] = g1;
     S->cs[j] = c;
     S->sn[j] = s;
-    double2 hjj = H[j * kM + j], hj1 = H[(j + 1) * kM + j];
-    double2 t1 = dmul(s, hj1);
-    H[j * kM + j] = make_double2(c * hjj.x + t1.x, c * hjj.y + t1.y);
-    H[(j + 1) * kM + j] = make_double2(0.0, 0.0);
-    double2 gj = S->g[j], gj1 = S->g[j + 1];
-    double2 t3 = dmul(s, gj1);
-    double2 t4 = dmul(make_double2(-s.x, s.y), gj);
-    S->g[j] = make_double2(c * gj.x + t3.x, c * gj.y + t3.y);
-    S->g[j + 1] = make_double2(t4.x + c * gj1.x, t4.y + c * gj1.y);
-    S->scal[2] = dabs(S->g[j + 1]);
+    S->scal[1] = hn;
+    const double gabs = dabs(g1);
+    S->scal[2] = gabs;
+    S->jdone = j + 1;
+    if (!isfinite(gabs)) {
+      S->bad = 1;
+      S->done = 1;
+    } else if (gabs < abs_tol || gabs < inner_thr) {
+      S->done = 1;
+    }
   }
+  __syncthreads();
+  if (t <= j + 1) S->H[t * kM + j] = sH[t];
 }
 
 // v_{j+1} = w / h_{j+1,j}, or 0 on a lucky breakdown (iterative.rs:101-106)
 __global__ void __launch_bounds__(kVecThreads)
 k_next_basis(int len, const double2* __restrict__ w, double2* __restrict__ vnext,
              const GmresState* S) {
+  if (S->done) return;  // the basis beyond a finished step is never used
   const double hn = S->scal[1];
   const bool ok = hn > 1e-30;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < len; q += gridDim.x * blockDim.x) {
@@ -235,24 +276,44 @@ k_next_basis(int len, const double2* __restrict__ w, double2* __restrict__ vnext
 }
 
 // Back substitution H[0..j,0..j] y = g[0..j] (iterative.rs:194-206).
-__global__ void k_backsub(int j, GmresState* S) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  for (int i = j - 1; i >= 0; --i) {
-    double2 sum = S->g[i];
-    for (int q = i + 1; q < j; ++q) {
-      double2 t = dmul(S->H[i * kM + q], S->y[q]);
-      sum.x -= t.x;
-      sum.y -= t.y;
-    }
-    double2 hii = S->H[i * kM + i];
-    S->y[i] = (dabs(hii) > 1e-30) ? ddiv(sum, hii) : make_double2(0.0, 0.0);
+// The leading j x j block of H and g[0..j) are staged in shared memory by
+// the whole block, then one thread substitutes.
+// Upper triangle packed row by row: row r holds columns r..j-1 at
+// tri_off(r) = r*j - r*(r-1)/2 (at most 64*65/2 entries, 33 KB).
+__device__ __forceinline__ int tri_off(int r, int j) { return r * j - (r * (r - 1)) / 2; }
+
+__global__ void __launch_bounds__(kVecThreads) k_backsub(GmresState* S) {
+  const int j = S->jdone;
+  __shared__ double2 sH[kM * (kM + 1) / 2];
+  __shared__ double2 sg[kM], sy[kM];
+  for (int e = threadIdx.x; e < j * j; e += blockDim.x) {
+    const int r = e / j, c = e % j;
+    if (c >= r) sH[tri_off(r, j) + (c - r)] = S->H[r * kM + c];
   }
+  if (threadIdx.x < j) sg[threadIdx.x] = S->g[threadIdx.x];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int i = j - 1; i >= 0; --i) {
+      double2 sum = sg[i];
+      const double2* row = sH + tri_off(i, j) - i;  // row[q] = H[i][q] for q >= i
+      for (int q = i + 1; q < j; ++q) {
+        const double2 t = dmul(row[q], sy[q]);
+        sum.x -= t.x;
+        sum.y -= t.y;
+      }
+      const double2 hii = row[i];
+      sy[i] = (dabs(hii) > 1e-30) ? ddiv(sum, hii) : make_double2(0.0, 0.0);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < j) S->y[threadIdx.x] = sy[threadIdx.x];
 }
 
 // x += sum_i y_i v_i (iterative.rs:142-144)
 __global__ void __launch_bounds__(kVecThreads)
-k_update_x(int len, double2* __restrict__ x, const double2* __restrict__ V, int j,
+k_update_x(int len, double2* __restrict__ x, const double2* __restrict__ V,
            const GmresState* S) {
+  const int j = S->jdone;
   __shared__ double2 ys[kM];
   if (threadIdx.x < j) ys[threadIdx.x] = S->y[threadIdx.x];
   __syncthreads();
@@ -302,8 +363,10 @@ lum_status vec_norm(const double2* v, int len, GmresWork& W, int slot, cudaStrea
 }
 
 lum_status read_scalars(GmresWork& W, cudaStream_t st) {
-  LUM_TRY_CUDA(cudaMemcpyAsync(W.h_state->scal, W.state.as<GmresState>()->scal,
-                               sizeof(double) * 8, cudaMemcpyDeviceToHost, st));
+  // scal[8] and the done/jdone/bad flags are contiguous at the end of the state
+  const size_t bytes = sizeof(GmresState) - offsetof(GmresState, scal);
+  LUM_TRY_CUDA(cudaMemcpyAsync(W.h_state->scal, W.state.as<GmresState>()->scal, bytes,
+                               cudaMemcpyDeviceToHost, st));
   LUM_TRY_CUDA(cudaStreamSynchronize(st));
   return LUM_OK;
 }
@@ -362,37 +425,28 @@ lum_status lum_gmres_device(lum_session* s, const double2* b, double2* x, double
       result = LUM_ERR_NOT_CONVERGED;
       break;
     }
+    // One restart cycle is enqueued whole: the device ends it early (S->done)
+    // when a step meets the test, and the host reads the outcome once, after
+    // the cycle's FP64 residual.  No host round trip per Arnoldi step.
+    const int jmax = std::min(m, max_iter - total);
+    const double inner_thr = (mode == LUM_SOLVE_FP32_REFINE) ? inner_rel * beta : 0.0;
+    const int* done = &S->done;
     k_start_cycle<<<nb, kVecThreads, 0, st>>>(len, r, V, S, m);
     LUM_CHECK_LAUNCH();
-    int j = 0;
-    while (j < m && total < max_iter) {
-      LUM_TRY(s->apply(arnoldi_prec, V + (size_t)j * len, w));
-      if (arnoldi_prec == LUM_FP32)
-        loc.matvecs_fp32++;
-      else
-        loc.matvecs_fp64++;
+    for (int j = 0; j < jmax; ++j) {
+      LUM_TRY(s->apply(arnoldi_prec, V + (size_t)j * len, w, done));
       for (int i = 0; i <= j; ++i) {
         k_mgs<<<nb, kVecThreads, 0, st>>>(len, w, V, i, j, parts, cnt, S);
         LUM_CHECK_LAUNCH();
       }
-      k_mgs_final<<<nb, kVecThreads, 0, st>>>(len, w, V, j, parts, cnt, S);
+      k_mgs_final<<<nb, kVecThreads, 0, st>>>(len, w, V, j, parts, cnt, S, abs_tol, inner_thr);
       LUM_CHECK_LAUNCH();
       k_next_basis<<<nb, kVecThreads, 0, st>>>(len, w, V + (size_t)(j + 1) * len, S);
       LUM_CHECK_LAUNCH();
-      LUM_TRY(read_scalars(W, st));
-      const double gabs = W.h_state->scal[2];
-      total++;
-      j++;
-      if (!std::isfinite(gabs)) {
-        set_error("GMRES breakdown: non-finite residual estimate");
-        return LUM_ERR_DEVICE;
-      }
-      if (gabs < abs_tol) break;
-      if (mode == LUM_SOLVE_FP32_REFINE && gabs < inner_rel * beta) break;
     }
-    k_backsub<<<1, 32, 0, st>>>(j, S);
+    k_backsub<<<1, kVecThreads, 0, st>>>(S);
     LUM_CHECK_LAUNCH();
-    k_update_x<<<nb, kVecThreads, 0, st>>>(len, x, V, j, S);
+    k_update_x<<<nb, kVecThreads, 0, st>>>(len, x, V, S);
     LUM_CHECK_LAUNCH();
     // true residual in FP64 (iterative.rs:147-151)
     LUM_TRY(s->apply(LUM_FP64, x, tmp));
@@ -400,6 +454,16 @@ lum_status lum_gmres_device(lum_session* s, const double2* b, double2* x, double
     k_residual<<<nb, kVecThreads, 0, st>>>(len, b, tmp, r, parts, cnt, S);
     LUM_CHECK_LAUNCH();
     LUM_TRY(read_scalars(W, st));
+    const int steps = W.h_state->jdone;
+    total += steps;
+    if (arnoldi_prec == LUM_FP32)
+      loc.matvecs_fp32 += steps;
+    else
+      loc.matvecs_fp64 += steps;
+    if (W.h_state->bad) {
+      set_error("GMRES breakdown: non-finite residual estimate");
+      return LUM_ERR_DEVICE;
+    }
     beta = W.h_state->scal[3];
     loc.restarts++;
     if (!std::isfinite(beta)) {

@@ -101,6 +101,8 @@ struct OtfOperator {
   double center[3] = {0, 0, 0};
   double extent = 0.0;      // bounding-box diagonal (nm)
   int fast_trig = 1;        // k*extent within the fast FP32 sincos range
+  int lofree = 0;           // every centred position is exact in FP32 (lo == 0)
+  int img_lofree = 0;       // same for the substrate image positions
 
   DevBuf pos64;             // double4[n]
   DevBuf pos_hi, pos_lo;    // float4[n] (centred)
@@ -114,14 +116,20 @@ struct OtfOperator {
   DevBuf lat_recip;         // double4[n_recip] reciprocal points
   DevBuf partial;           // scratch: FP32 or FP64 partial sums [nsplit][3n]
   int nsplit32 = 1, nsplit64 = 1;
+  int f32_variant = 0;      // FP32 pair-kernel variant chosen by the tuner
+  int nsplit_v[8] = {1, 1, 1, 1, 1, 1, 1, 1};
+  float tuned_ms = 0.f;     // tuned FP32 pair-kernel time (ms), 0 if untuned
+  lum_status tune_f32(cudaStream_t st);
   std::vector<double> host_pos;  // double4 host copy (image positions are built from it)
 
   lum_status build_geometry(const double* pos_host, int n, cudaStream_t st);
   lum_status set_physics(double k, const double* inv_alpha_host, int use_fcd, double cell,
                          const lum_lattice* lat, const double* kb, const lum_substrate* sub,
                          cudaStream_t st);
+  // skip: optional device flag; when it is nonzero at kernel start every
+  // kernel of this application returns at once (y is left untouched).
   lum_status apply(int precision, const double2* x, double2* y, cudaStream_t st,
-                   cudaEvent_t ev0, cudaEvent_t ev1);
+                   cudaEvent_t ev0, cudaEvent_t ev1, const int* skip = nullptr);
 };
 
 // --- cached (dense matrix) operator ----------------------------------------
@@ -133,7 +141,7 @@ struct CachedOperator {
   lum_status allocate(int dim, int precision);
   lum_status upload(const double* host, cudaStream_t st);
   lum_status assemble(const OtfOperator& geo, cudaStream_t st);
-  lum_status apply(const double2* x, double2* y, cudaStream_t st);
+  lum_status apply(const double2* x, double2* y, cudaStream_t st, const int* skip = nullptr);
   lum_status apply_multi(const double2* X, double2* Y, int nrhs, cudaStream_t st);
 };
 
@@ -145,6 +153,10 @@ struct GmresState {
   double2 g[kMaxRestart + 1];
   double2 y[kMaxRestart];
   double scal[8];   // 0: last norm, 1: h_{j+1,j}, 2: |g[j+1]|, 3: residual norm
+  int done;         // the cycle has met its test: later kernels of the cycle exit at once
+  int jdone;        // Arnoldi steps completed in the current cycle
+  int bad;          // a non-finite residual estimate was produced
+  int pad;
 };
 
 struct GmresWork {
@@ -156,6 +168,8 @@ struct GmresWork {
   lum_status ensure(int len, int m, cudaStream_t st);
   ~GmresWork();
 };
+
+const char* f32_variant_name(int v);  // otf.cu
 
 // vector kernels (gmres.cu)
 lum_status vec_norm(const double2* v, int len, GmresWork& W, int slot, cudaStream_t st);
@@ -190,5 +204,5 @@ struct lum_session {
   };
   std::vector<EvRec> ev_pool;
   size_t ev_used = 0;
-  lum_status apply(int precision, const double2* x, double2* y);
+  lum_status apply(int precision, const double2* x, double2* y, const int* skip = nullptr);
 };

@@ -30,110 +30,17 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <cstdlib>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 namespace lum {
 
 constexpr int kOtfBlock = 128;
-
-// ---------------------------------------------------------------------------
-// FP32 dense pair kernel
-// ---------------------------------------------------------------------------
-// Source tile entry: P0 = (hx, hy, hz, lx), P1 = (ly, lz, x0r, x0i),
-// P2 = (x1r, x1i, x2r, x2i)  -- 3 x LDS.128 per source.
-template <bool FAST, bool IMAGE, int R>
-__global__ void __launch_bounds__(kOtfBlock)
-otf_pairs_f32(int n, const float4* __restrict__ obs_hi, const float4* __restrict__ obs_lo,
-              const float4* __restrict__ src_hi, const float4* __restrict__ src_lo,
-              const double2* __restrict__ x, float2 m0, float2 m1, float2 m2, float k,
-              float inv_k, float s0, int chunk, float2* __restrict__ partial) {
-  __shared__ float4 sP0[kOtfBlock], sP1[kOtfBlock], sP2[kOtfBlock];
-  const int tid = threadIdx.x;
-  int irow[R];
-  float ohx[R], ohy[R], ohz[R], olx[R], oly[R], olz[R];
-  float acc[R][6];
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    int i = blockIdx.x * (kOtfBlock * R) + r * kOtfBlock + tid;
-    irow[r] = i;
-    int ic = min(i, n - 1);
-    float4 h = obs_hi[ic], l = obs_lo[ic];
-    ohx[r] = h.x; ohy[r] = h.y; ohz[r] = h.z;
-    olx[r] = l.x; oly[r] = l.y; olz[r] = l.z;
-#pragma unroll
-    for (int c = 0; c < 6; ++c) acc[r][c] = 0.f;
-  }
-  const int j_begin = blockIdx.y * chunk;
-  const int j_end = min(n, j_begin + chunk);
-  for (int jt = j_begin; jt < j_end; jt += kOtfBlock) {
-    const int cnt = min(kOtfBlock, j_end - jt);
-    __syncthreads();
-    if (tid < cnt) {
-      const int j = jt + tid;
-      float4 h = src_hi[j], l = src_lo[j];
-      double2 a = x[3 * j], b = x[3 * j + 1], c = x[3 * j + 2];
-      float2 xa = make_float2((float)a.x, (float)a.y);
-      float2 xb = make_float2((float)b.x, (float)b.y);
-      float2 xc = make_float2((float)c.x, (float)c.y);
-      if (IMAGE) {  // x'_b = m_b x_b, m = (-r, -r, +r)  (assembly.rs:288-292)
-        xa = make_float2(m0.x * xa.x - m0.y * xa.y, m0.x * xa.y + m0.y * xa.x);
-        xb = make_float2(m1.x * xb.x - m1.y * xb.y, m1.x * xb.y + m1.y * xb.x);
-        xc = make_float2(m2.x * xc.x - m2.y * xc.y, m2.x * xc.y + m2.y * xc.x);
-      }
-      sP0[tid] = make_float4(h.x, h.y, h.z, l.x);
-      sP1[tid] = make_float4(l.y, l.z, xa.x, xa.y);
-      sP2[tid] = make_float4(xb.x, xb.y, xc.x, xc.y);
-    }
-    __syncthreads();
-#pragma unroll 2
-    for (int jj = 0; jj < cnt; ++jj) {
-      const float4 P0 = sP0[jj], P1 = sP1[jj], P2 = sP2[jj];
-      const int j = jt + jj;
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        float dx = (ohx[r] - P0.x) + (olx[r] - P0.w);
-        float dy = (ohy[r] - P0.y) + (oly[r] - P1.x);
-        float dz = (ohz[r] - P0.z) + (olz[r] - P1.y);
-        float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-        bool skip = IMAGE ? (r2 < 1e-20f) : (j == irow[r]);
-        if (skip) r2 = 1.0f;
-        float ir = rsqrtf(r2);
-        float Rr = r2 * ir;
-        float u = ir * inv_k;
-        float u2 = u * u;
-        float sn, cs;
-        if (FAST)
-          __sincosf(k * Rr, &sn, &cs);
-        else
-          sincosf(k * Rr, &sn, &cs);
-        float su = skip ? 0.f : s0 * u;
-        float pr = su * cs, pi = su * sn;
-        float ar = 1.0f - u2;
-        float Ar = fmaf(pr, ar, -pi * u), Ai = fmaf(pr, u, pi * ar);
-        float br = fmaf(3.0f, u2, -1.0f), bi = -3.0f * u;
-        float ir2 = ir * ir;
-        float Br = fmaf(pr, br, -pi * bi) * ir2, Bi = fmaf(pr, bi, pi * br) * ir2;
-        float dxr = fmaf(dx, P1.z, fmaf(dy, P2.x, dz * P2.z));
-        float dxi = fmaf(dx, P1.w, fmaf(dy, P2.y, dz * P2.w));
-        float tr = fmaf(Br, dxr, -Bi * dxi), ti = fmaf(Br, dxi, Bi * dxr);
-        acc[r][0] = fmaf(tr, dx, fmaf(Ar, P1.z, fmaf(-Ai, P1.w, acc[r][0])));
-        acc[r][1] = fmaf(ti, dx, fmaf(Ar, P1.w, fmaf(Ai, P1.z, acc[r][1])));
-        acc[r][2] = fmaf(tr, dy, fmaf(Ar, P2.x, fmaf(-Ai, P2.y, acc[r][2])));
-        acc[r][3] = fmaf(ti, dy, fmaf(Ar, P2.y, fmaf(Ai, P2.x, acc[r][3])));
-        acc[r][4] = fmaf(tr, dz, fmaf(Ar, P2.z, fmaf(-Ai, P2.w, acc[r][4])));
-        acc[r][5] = fmaf(ti, dz, fmaf(Ar, P2.w, fmaf(Ai, P2.z, acc[r][5])));
-      }
-    }
-  }
-  float2* out = partial + (size_t)blockIdx.y * (3 * (size_t)n);
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    if (irow[r] < n) {
-      out[3 * irow[r] + 0] = make_float2(acc[r][0], acc[r][1]);
-      out[3 * irow[r] + 1] = make_float2(acc[r][2], acc[r][3]);
-      out[3 * irow[r] + 2] = make_float2(acc[r][4], acc[r][5]);
-    }
-  }
-}
+}  // namespace lum
+#include "pairs_f32x2.cuh"
+namespace lum {
 
 // ---------------------------------------------------------------------------
 // FP64 dense pair kernel (same decomposition; sources as double4 + 3 double2)
@@ -142,7 +49,9 @@ template <bool IMAGE>
 __global__ void __launch_bounds__(kOtfBlock)
 otf_pairs_f64(int n, const double4* __restrict__ pos, const double2* __restrict__ x,
               double2 m0, double2 m1, double2 m2, double z_mirror, double k, double inv_k,
-              double s0, int chunk, double2* __restrict__ partial) {
+              double s0, int chunk, double2* __restrict__ partial,
+              const int* __restrict__ skip) {
+  if (skip && *skip) return;
   __shared__ double4 sP[kOtfBlock];
   __shared__ double2 sX[3 * kOtfBlock];
   const int tid = threadIdx.x;
@@ -215,31 +124,25 @@ otf_pairs_f64(int n, const double4* __restrict__ pos, const double2* __restrict_
 __device__ __forceinline__ double2 to_d2(float2 v) { return make_double2(v.x, v.y); }
 __device__ __forceinline__ double2 to_d2(double2 v) { return v; }
 
+// kEpiTPR consecutive threads share one dipole: they split the pair partials
+// and the near-pair slots between them (more loads in flight per row), then
+// combine by shuffle in a fixed order; the first thread adds alpha^-1 x.
+constexpr int kEpiTPR = 4;
+
 template <typename TP, typename TC>
 __global__ void __launch_bounds__(256)
 otf_epilogue(int n, const double2* __restrict__ x, const double2* __restrict__ inv_alpha,
              const TP* __restrict__ partial, int nparts, int ell_w,
              const int* __restrict__ near_j, const TC* __restrict__ fcd,
-             double2* __restrict__ y) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  double2 xi[3] = {x[3 * i], x[3 * i + 1], x[3 * i + 2]};
-  double yr[3], yi[3];
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    double sr = 0.0, si = 0.0;
-#pragma unroll
-    for (int b = 0; b < 3; ++b) {
-      double2 m = inv_alpha[(size_t)(3 * a + b) * n + i];
-      sr += m.x * xi[b].x - m.y * xi[b].y;
-      si += m.x * xi[b].y + m.y * xi[b].x;
-    }
-    yr[a] = sr;
-    yi[a] = si;
-  }
+             double2* __restrict__ y, const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = min(gid / kEpiTPR, n - 1);
+  const int sub = gid % kEpiTPR;
+  const bool live = gid / kEpiTPR < n;
   double gr[3] = {0, 0, 0}, gi[3] = {0, 0, 0};
   const size_t stride = 3 * (size_t)n;
-  for (int s = 0; s < nparts; ++s) {
+  for (int s = sub; s < nparts; s += kEpiTPR) {
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       double2 p = to_d2(partial[s * stride + 3 * i + a]);
@@ -247,9 +150,9 @@ otf_epilogue(int n, const double2* __restrict__ x, const double2* __restrict__ i
       gi[a] += p.y;
     }
   }
-  for (int w = 0; w < ell_w; ++w) {
+  for (int w = sub; w < ell_w; w += kEpiTPR) {
     const int j = near_j[(size_t)w * n + i];
-    if (j < 0) break;
+    if (j < 0) break;  // lists are packed: the rest of this row is padding
     double2 xj[3] = {x[3 * j], x[3 * j + 1], x[3 * j + 2]};
 #pragma unroll
     for (int a = 0; a < 3; ++a)
@@ -261,7 +164,25 @@ otf_epilogue(int n, const double2* __restrict__ x, const double2* __restrict__ i
       }
   }
 #pragma unroll
-  for (int a = 0; a < 3; ++a) y[3 * i + a] = make_double2(yr[a] - gr[a], yi[a] - gi[a]);
+  for (int o = 1; o < kEpiTPR; o <<= 1)
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      gr[a] += __shfl_xor_sync(0xffffffffu, gr[a], o);
+      gi[a] += __shfl_xor_sync(0xffffffffu, gi[a], o);
+    }
+  if (!live || sub != 0) return;
+  const double2 xi[3] = {x[3 * i], x[3 * i + 1], x[3 * i + 2]};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    double sr = 0.0, si = 0.0;
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      double2 m = inv_alpha[(size_t)(3 * a + b) * n + i];
+      sr += m.x * xi[b].x - m.y * xi[b].y;
+      si += m.x * xi[b].y + m.y * xi[b].x;
+    }
+    y[3 * i + a] = make_double2(sr - gr[a], si - gi[a]);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -368,7 +289,8 @@ otf_pairs_ewald(int n, const double4* __restrict__ pos, const double2* __restric
                 LatticeDev L, const double4* __restrict__ lreal,
                 const double4* __restrict__ lrecip, double kb0, double kb1, double kb2,
                 double k, int has_sub, SubstrateDev sub, int chunk,
-                double2* __restrict__ partial) {
+                double2* __restrict__ partial, const int* __restrict__ skip) {
+  if (skip && *skip) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double kb[3] = {kb0, kb1, kb2};
@@ -441,9 +363,73 @@ int choose_nsplit(int rowblocks, int ntiles, int ctas_per_sm, int sms) {
   return best;
 }
 
-constexpr int kRowsF32 = 2;
+// FP32 pair-kernel variants the tuner chooses from: rows per thread (2*RP)
+// and the register cap implied by MINB resident CTAs per SM.
+struct F32Args {
+  int n;
+  const float4 *oh, *ol, *sh, *sl;
+  const double2* x;
+  float2 m0, m1, m2;
+  float k, ik, s0;
+  int chunk;
+  float2* part;
+  const int* skip;
+};
+
+template <int RP, int MINB>
+struct F32Variant {
+  template <bool IMAGE>
+  static void launch(int fast, int lofree, dim3 grid, cudaStream_t st, const F32Args& a) {
+#define LUM_F32_LAUNCH(F, L)                                                                  \
+  otf_pairs_f32<F, IMAGE, L, RP, MINB><<<grid, kOtfBlock, 0, st>>>(                           \
+      a.n, a.oh, a.ol, a.sh, a.sl, a.x, a.m0, a.m1, a.m2, a.k, a.ik, a.s0, a.chunk, a.part, \
+      a.skip)
+    if (fast && lofree)
+      LUM_F32_LAUNCH(true, true);
+    else if (fast)
+      LUM_F32_LAUNCH(true, false);
+    else if (lofree)
+      LUM_F32_LAUNCH(false, true);
+    else
+      LUM_F32_LAUNCH(false, false);
+#undef LUM_F32_LAUNCH
+  }
+  static int occupancy(int fast, int lofree) {
+    int occ = 1;
+    if (fast && lofree)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, otf_pairs_f32<true, false, true, RP, MINB>, kOtfBlock, 0);
+    else if (fast)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, otf_pairs_f32<true, false, false, RP, MINB>, kOtfBlock, 0);
+    else if (lofree)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, otf_pairs_f32<false, false, true, RP, MINB>, kOtfBlock, 0);
+    else
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, otf_pairs_f32<false, false, false, RP, MINB>, kOtfBlock, 0);
+    return std::max(1, occ);
+  }
+};
+
+struct F32VariantEntry {
+  const char* name;
+  int rows;  // observer rows per thread
+  void (*direct)(int, int, dim3, cudaStream_t, const F32Args&);
+  void (*image)(int, int, dim3, cudaStream_t, const F32Args&);
+  int (*occupancy)(int, int);
+};
+
+const F32VariantEntry kF32Variants[] = {
+    {"rows2_minb1", 2, F32Variant<1, 1>::launch<false>, F32Variant<1, 1>::launch<true>, F32Variant<1, 1>::occupancy},
+    {"rows2_minb6", 2, F32Variant<1, 6>::launch<false>, F32Variant<1, 6>::launch<true>, F32Variant<1, 6>::occupancy},
+    {"rows2_minb8", 2, F32Variant<1, 8>::launch<false>, F32Variant<1, 8>::launch<true>, F32Variant<1, 8>::occupancy},
+    {"rows4_minb3", 4, F32Variant<2, 3>::launch<false>, F32Variant<2, 3>::launch<true>, F32Variant<2, 3>::occupancy},
+    {"rows4_minb4", 4, F32Variant<2, 4>::launch<false>, F32Variant<2, 4>::launch<true>, F32Variant<2, 4>::occupancy},
+};
+constexpr int kNumF32Variants = sizeof(kF32Variants) / sizeof(kF32Variants[0]);
 
 }  // namespace
+
+const char* f32_variant_name(int v) {
+  return (v >= 0 && v < kNumF32Variants) ? kF32Variants[v].name : "none";
+}
 
 lum_status OtfOperator::build_geometry(const double* pos_host, int n_, cudaStream_t st) {
   n = n_;
@@ -489,6 +475,12 @@ lum_status OtfOperator::build_geometry(const double* pos_host, int n_, cudaStrea
   LUM_TRY_CUDA(cudaMemcpyAsync(pos_hi.p, h4.data(), pos_hi.bytes, cudaMemcpyHostToDevice, st));
   LUM_TRY_CUDA(cudaMemcpyAsync(pos_lo.p, l4.data(), pos_lo.bytes, cudaMemcpyHostToDevice, st));
   host_pos.swap(p4);
+  lofree = 1;
+  for (float v : l4)
+    if (v != 0.0f) {
+      lofree = 0;
+      break;
+    }
   return LUM_OK;
 }
 
@@ -647,6 +639,12 @@ lum_status OtfOperator::set_physics(double k_, const double* inv_alpha_host, int
       LUM_TRY(img_hi.alloc(sizeof(float) * 4 * (size_t)n));
       LUM_TRY(img_lo.alloc(sizeof(float) * 4 * (size_t)n));
     }
+    img_lofree = 1;
+    for (float v : l4)
+      if (v != 0.0f) {
+        img_lofree = 0;
+        break;
+      }
     LUM_TRY_CUDA(cudaMemcpyAsync(img_hi.p, h4.data(), img_hi.bytes, cudaMemcpyHostToDevice, st));
     LUM_TRY_CUDA(cudaMemcpyAsync(img_lo.p, l4.data(), img_lo.bytes, cudaMemcpyHostToDevice, st));
   }
@@ -667,34 +665,108 @@ lum_status OtfOperator::set_physics(double k_, const double* inv_alpha_host, int
                                                    fcd64.as<double2>(), fcd32.as<float2>());
     LUM_CHECK_LAUNCH();
   }
+  const int old_fast = fast_trig;
   fast_trig = (k * extent < 3.0) ? 1 : 0;
-  // partial-sum scratch
+  // partial-sum scratch, sized for the largest split of any FP32 variant
   if (first) {
-    int sms = device_sms();
-    int occ32 = 1, occ64 = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ32, otf_pairs_f32<true, false, kRowsF32>,
-                                                  kOtfBlock, 0);
+    const int sms = device_sms();
+    const int ntiles = (n + kOtfBlock - 1) / kOtfBlock;
+    size_t max_parts32 = 1;
+    for (int v = 0; v < kNumF32Variants; ++v) {
+      const int rows = kF32Variants[v].rows;
+      const int occ = kF32Variants[v].occupancy(1, lofree);
+      const int rb = (n + kOtfBlock * rows - 1) / (kOtfBlock * rows);
+      nsplit_v[v] = choose_nsplit(rb, ntiles, occ, sms);
+      max_parts32 = std::max<size_t>(max_parts32, nsplit_v[v]);
+    }
+    int occ64 = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ64, otf_pairs_f64<false>, kOtfBlock, 0);
-    int ntiles = (n + kOtfBlock - 1) / kOtfBlock;
-    int rb32 = (n + kOtfBlock * kRowsF32 - 1) / (kOtfBlock * kRowsF32);
-    int rb64 = ntiles;
-    nsplit32 = choose_nsplit(rb32, ntiles, std::max(1, occ32), sms);
-    nsplit64 = choose_nsplit(rb64, ntiles, std::max(1, occ64), sms);
-    int parts = std::max(nsplit32 * 2, nsplit64 * 2 + 0);
-    if (has_lattice) parts = std::max(parts, nsplit64);
-    size_t bytes = std::max(sizeof(float2) * (size_t)nsplit32 * 2, sizeof(double2) * (size_t)nsplit64 * 2) *
-                   3 * (size_t)n;
-    (void)parts;
+    nsplit64 = choose_nsplit(ntiles, ntiles, std::max(1, occ64), sms);
+    const size_t bytes = std::max(sizeof(float2) * max_parts32 * 2,
+                                  sizeof(double2) * (size_t)nsplit64 * 2) * 3 * (size_t)n;
     LUM_TRY(partial.alloc(bytes));
   }
+  if (first || old_fast != fast_trig) LUM_TRY(tune_f32(st));
+  return LUM_OK;
+}
+
+// Autotuner of the FP32 pair kernel: every variant (rows per thread x
+// register cap, with its own wave-filling split) is timed on this geometry
+// and the fastest is kept.  Choices are cached for the process per
+// (N, trig flavour, lo-free); LUMINA_TUNE=0 keeps the first variant.
+namespace {
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int>, int> g_tune_cache;
+}  // namespace
+
+lum_status OtfOperator::tune_f32(cudaStream_t st) {
+  f32_variant = 0;
+  const char* env = std::getenv("LUMINA_TUNE");
+  if ((env && env[0] == '0') || n < 2048) {
+    nsplit32 = nsplit_v[0];
+    return LUM_OK;
+  }
+  const auto key = std::make_tuple(n, fast_trig, lofree);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      f32_variant = it->second;
+      nsplit32 = nsplit_v[f32_variant];
+      return LUM_OK;
+    }
+  }
+  DevBuf xz;
+  LUM_TRY(xz.alloc(sizeof(double2) * 3 * (size_t)n));
+  LUM_TRY_CUDA(cudaMemsetAsync(xz.p, 0, xz.bytes, st));
+  cudaEvent_t e0, e1;
+  LUM_TRY_CUDA(cudaEventCreate(&e0));
+  LUM_TRY_CUDA(cudaEventCreate(&e1));
+  const int ntiles = (n + kOtfBlock - 1) / kOtfBlock;
+  const double s0 = k * k * k / (4.0 * kPi);
+  float best = 1e30f;
+  for (int v = 0; v < kNumF32Variants; ++v) {
+    const int rows = kF32Variants[v].rows, ns = nsplit_v[v];
+    const int chunk = ((ntiles + ns - 1) / ns) * kOtfBlock;
+    dim3 grid((n + kOtfBlock * rows - 1) / (kOtfBlock * rows), ns);
+    F32Args a{n, pos_hi.as<float4>(), pos_lo.as<float4>(), pos_hi.as<float4>(),
+              pos_lo.as<float4>(), xz.as<double2>(), make_float2(1.f, 0.f),
+              make_float2(1.f, 0.f), make_float2(1.f, 0.f), (float)k, (float)(1.0 / k),
+              (float)s0, chunk, partial.as<float2>(), nullptr};
+    float ms = 0.f;
+    for (int rep = 0; rep < 2; ++rep) {  // first launch warms, second is timed
+      cudaEventRecord(e0, st);
+      kF32Variants[v].direct(fast_trig, lofree, grid, st, a);
+      cudaEventRecord(e1, st);
+    }
+    cudaError_t e = cudaEventSynchronize(e1);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      return cuda_status(e, "pair-kernel tuning", __FILE__, __LINE__);
+    }
+    g_launches.fetch_add(2, std::memory_order_relaxed);
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best) {
+      best = ms;
+      f32_variant = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  nsplit32 = nsplit_v[f32_variant];
+  tuned_ms = best;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune_cache[key] = f32_variant;
   return LUM_OK;
 }
 
 lum_status OtfOperator::apply(int precision, const double2* x, double2* y, cudaStream_t st,
-                              cudaEvent_t ev0, cudaEvent_t ev1) {
+                              cudaEvent_t ev0, cudaEvent_t ev1, const int* skip) {
   const int ntiles = (n + kOtfBlock - 1) / kOtfBlock;
   const double s0 = k * k * k / (4.0 * kPi);
-  const int epi_blocks = (n + 255) / 256;
+  const int epi_blocks = (int)(((size_t)n * kEpiTPR + 255) / 256);
   if (has_lattice) {
     // Ewald path: FP64 pair kernel for either precision.
     const int ns = nsplit64;
@@ -704,53 +776,48 @@ lum_status OtfOperator::apply(int precision, const double2* x, double2* y, cudaS
     otf_pairs_ewald<<<grid, kOtfBlock, 0, st>>>(
         n, pos64.as<double4>(), x, latdev, lat_real.as<double4>(), lat_recip.as<double4>(),
         kbloch[0], kbloch[1], kbloch[2], k, has_substrate, substrate, chunk,
-        partial.as<double2>());
+        partial.as<double2>(), skip);
     LUM_CHECK_LAUNCH();
     if (ev1) cudaEventRecord(ev1, st);
     otf_epilogue<double2, double2><<<epi_blocks, 256, 0, st>>>(
-        n, x, inv_alpha.as<double2>(), partial.as<double2>(), ns, 0, nullptr, nullptr, y);
+        n, x, inv_alpha.as<double2>(), partial.as<double2>(), ns, 0, nullptr, nullptr, y, skip);
     LUM_CHECK_LAUNCH();
     return LUM_OK;
   }
   const double2 rr = make_double2(substrate.refl_re, substrate.refl_im);
   if (precision == LUM_FP32) {
+    const F32VariantEntry& V = kF32Variants[f32_variant];
     const int ns = nsplit32;
     const int chunk = ((ntiles + ns - 1) / ns) * kOtfBlock;
-    const int rb = (n + kOtfBlock * kRowsF32 - 1) / (kOtfBlock * kRowsF32);
+    const int rb = (n + kOtfBlock * V.rows - 1) / (kOtfBlock * V.rows);
     dim3 grid(rb, ns);
     const float kf = (float)k, ikf = (float)(1.0 / k), s0f = (float)s0;
     const float2 one = make_float2(1.f, 0.f);
     float2* part = partial.as<float2>();
+    F32Args a{n, pos_hi.as<float4>(), pos_lo.as<float4>(), pos_hi.as<float4>(),
+              pos_lo.as<float4>(), x, one, one, one, kf, ikf, s0f, chunk, part, skip};
     if (ev0) cudaEventRecord(ev0, st);
-    if (fast_trig)
-      otf_pairs_f32<true, false, kRowsF32><<<grid, kOtfBlock, 0, st>>>(
-          n, pos_hi.as<float4>(), pos_lo.as<float4>(), pos_hi.as<float4>(), pos_lo.as<float4>(),
-          x, one, one, one, kf, ikf, s0f, chunk, part);
-    else
-      otf_pairs_f32<false, false, kRowsF32><<<grid, kOtfBlock, 0, st>>>(
-          n, pos_hi.as<float4>(), pos_lo.as<float4>(), pos_hi.as<float4>(), pos_lo.as<float4>(),
-          x, one, one, one, kf, ikf, s0f, chunk, part);
+    V.direct(fast_trig, lofree, grid, st, a);
     LUM_CHECK_LAUNCH();
     if (ev1) cudaEventRecord(ev1, st);
     int nparts = ns;
     if (has_substrate) {
       const float2 mneg = make_float2((float)-rr.x, (float)-rr.y);
       const float2 mpos = make_float2((float)rr.x, (float)rr.y);
-      float2* part2 = part + (size_t)ns * 3 * n;
-      if (fast_trig)
-        otf_pairs_f32<true, true, kRowsF32><<<grid, kOtfBlock, 0, st>>>(
-            n, pos_hi.as<float4>(), pos_lo.as<float4>(), img_hi.as<float4>(),
-            img_lo.as<float4>(), x, mneg, mneg, mpos, kf, ikf, s0f, chunk, part2);
-      else
-        otf_pairs_f32<false, true, kRowsF32><<<grid, kOtfBlock, 0, st>>>(
-            n, pos_hi.as<float4>(), pos_lo.as<float4>(), img_hi.as<float4>(),
-            img_lo.as<float4>(), x, mneg, mneg, mpos, kf, ikf, s0f, chunk, part2);
+      F32Args b = a;
+      b.sh = img_hi.as<float4>();
+      b.sl = img_lo.as<float4>();
+      b.m0 = mneg;
+      b.m1 = mneg;
+      b.m2 = mpos;
+      b.part = part + (size_t)ns * 3 * n;
+      V.image(fast_trig, lofree && img_lofree, grid, st, b);
       LUM_CHECK_LAUNCH();
       nparts = 2 * ns;
     }
     otf_epilogue<float2, float2><<<epi_blocks, 256, 0, st>>>(
         n, x, inv_alpha.as<double2>(), part, nparts, ell_w, near_j.as<int>(),
-        fcd32.as<float2>(), y);
+        fcd32.as<float2>(), y, skip);
     LUM_CHECK_LAUNCH();
     return LUM_OK;
   }
@@ -762,7 +829,7 @@ lum_status OtfOperator::apply(int precision, const double2* x, double2* y, cudaS
   double2* part = partial.as<double2>();
   if (ev0) cudaEventRecord(ev0, st);
   otf_pairs_f64<false><<<grid, kOtfBlock, 0, st>>>(n, pos64.as<double4>(), x, one, one, one, 0.0,
-                                                   k, 1.0 / k, s0, chunk, part);
+                                                   k, 1.0 / k, s0, chunk, part, skip);
   LUM_CHECK_LAUNCH();
   if (ev1) cudaEventRecord(ev1, st);
   int nparts = ns;
@@ -770,13 +837,13 @@ lum_status OtfOperator::apply(int precision, const double2* x, double2* y, cudaS
     const double2 mneg = make_double2(-rr.x, -rr.y);
     otf_pairs_f64<true><<<grid, kOtfBlock, 0, st>>>(
         n, pos64.as<double4>(), x, mneg, mneg, rr, 2.0 * substrate.z_interface, k, 1.0 / k, s0,
-        chunk, part + (size_t)ns * 3 * n);
+        chunk, part + (size_t)ns * 3 * n, skip);
     LUM_CHECK_LAUNCH();
     nparts = 2 * ns;
   }
   otf_epilogue<double2, double2><<<epi_blocks, 256, 0, st>>>(
       n, x, inv_alpha.as<double2>(), part, nparts, ell_w, near_j.as<int>(),
-      fcd64.as<double2>(), y);
+      fcd64.as<double2>(), y, skip);
   LUM_CHECK_LAUNCH();
   return LUM_OK;
 }

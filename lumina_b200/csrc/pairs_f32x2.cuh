@@ -1,0 +1,214 @@
+// pairs_f32x2.cuh -- FP32 dense pair kernel with packed f32x2 arithmetic.
+//
+// Each thread owns 2*RP observer dipoles.  Rows are packed in pairs into the
+// two halves of a float2, and every scalar step of the pair interaction runs
+// as one sm_100 f32x2 instruction (__ffma2_rn / __fmul2_rn / __fadd2_rn) for
+// both rows.  The kernel was issue-bound (~78 instructions per pair at 87 %
+// issue utilisation); packing halves the issue count, so the FP32 pipe
+// becomes the limit.  Only the rsqrt and sin/cos (MUFU) stay per row.
+//
+// Shared source tile, 6 x float4 per source, each value duplicated so that
+// one broadcast LDS.128 yields two (v, v) pairs:
+//   S0 = (hx,hx,hy,hy)  S1 = (hz,hz,x0r,x0r)  S2 = (x0i,x0i,x1r,x1r)
+//   S3 = (x1i,x1i,x2r,x2r)  S4 = (x2i,x2i,lx,lx)  S5 = (ly,ly,lz,lz)
+// LOFREE skips S5 and the lo terms when every centred position is exact in
+// FP32 (lo == 0), e.g. a lattice whose coordinates are multiples of 2^-k.
+//
+// The self pair (j == i) only occurs in the two tiles that hold the CTA's
+// own rows; only those tiles run the masked loop.  The substrate image pass
+// (IMAGE) masks pairs whose image distance is below 1e-10 nm (r^2 < 1e-20).
+#pragma once
+
+namespace lum {
+
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 lo2(const float4& v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ float2 hi2(const float4& v) { return make_float2(v.z, v.w); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+// a - b as one FMA: b * (-1) + a is exact-rounded like the subtraction
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
+  return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a);
+}
+
+template <bool FAST, bool IMAGE, bool LOFREE, bool CHECKED, int RP>
+__device__ __forceinline__ void pair_tile_f32x2(
+    const float4 (*__restrict__ sS)[kOtfBlock], int cnt, int jt, const int* irow,
+    const float2* OX, const float2* OY, const float2* OZ, const float2* LX, const float2* LY,
+    const float2* LZ, float2 (*acc)[6], float k, float2 inv_k2, float2 s02, float2 k2) {
+#pragma unroll 2
+  for (int jj = 0; jj < cnt; ++jj) {
+    const float4 S0 = sS[0][jj], S1 = sS[1][jj], S2 = sS[2][jj], S3 = sS[3][jj], S4 = sS[4][jj];
+    float4 S5 = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (!LOFREE) S5 = sS[5][jj];
+    const float2 x0r = hi2(S1), x0i = lo2(S2), x1r = hi2(S2), x1i = lo2(S3), x2r = hi2(S3),
+                 x2i = lo2(S4);
+    const int j = jt + jj;
+#pragma unroll
+    for (int p = 0; p < RP; ++p) {
+      float2 dx = sub2(OX[p], lo2(S0));
+      float2 dy = sub2(OY[p], hi2(S0));
+      float2 dz = sub2(OZ[p], lo2(S1));
+      if (!LOFREE) {
+        dx = add2(dx, sub2(LX[p], hi2(S4)));
+        dy = add2(dy, sub2(LY[p], lo2(S5)));
+        dz = add2(dz, sub2(LZ[p], hi2(S5)));
+      }
+      float2 r2 = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
+      float2 keep = make_float2(1.0f, 1.0f);
+      if (CHECKED) {
+        const bool sx = IMAGE ? (r2.x < 1e-20f) : (j == irow[2 * p]);
+        const bool sy = IMAGE ? (r2.y < 1e-20f) : (j == irow[2 * p + 1]);
+        if (sx) { r2.x = 1.0f; keep.x = 0.0f; }
+        if (sy) { r2.y = 1.0f; keep.y = 0.0f; }
+      }
+      const float2 ir = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+      const float2 kR = mul2(mul2(r2, ir), k2);          // k R
+      float2 sn, cs;
+      if (FAST) {
+        __sincosf(kR.x, &sn.x, &cs.x);
+        __sincosf(kR.y, &sn.y, &cs.y);
+      } else {
+        sincosf(kR.x, &sn.x, &cs.x);
+        sincosf(kR.y, &sn.y, &cs.y);
+      }
+      const float2 u = mul2(ir, inv_k2);                 // 1/(kR)
+      const float2 u2 = mul2(u, u);
+      float2 q = mul2(s02, u);                           // k^3/(4 pi) u
+      if (CHECKED) q = mul2(q, keep);
+      const float2 pr = mul2(q, cs), pi = mul2(q, sn);   // pf = pr + i pi
+      const float2 ar = sub2(make_float2(1.0f, 1.0f), u2);
+      // A = pf a,  a = 1 - u^2 + i u
+      const float2 Ar = sub2(mul2(pr, ar), mul2(pi, u));
+      const float2 Ai = fma2(pr, u, mul2(pi, ar));
+      // B' = pf b / R^2 with b = 3u^2 - 1 - 3iu = 2 - 3a, so B' = (2 pf - 3 A) ir^2
+      const float2 m3 = make_float2(-3.0f, -3.0f);
+      const float2 ir2 = mul2(ir, ir);
+      const float2 Br = mul2(fma2(Ar, m3, add2(pr, pr)), ir2);
+      const float2 Bi = mul2(fma2(Ai, m3, add2(pi, pi)), ir2);
+      // d . x_j
+      const float2 dxr = fma2(dx, x0r, fma2(dy, x1r, mul2(dz, x2r)));
+      const float2 dxi = fma2(dx, x0i, fma2(dy, x1i, mul2(dz, x2i)));
+      const float2 tr = sub2(mul2(Br, dxr), mul2(Bi, dxi));
+      const float2 ti = fma2(Br, dxi, mul2(Bi, dxr));
+      const float2 nAi = mul2(Ai, make_float2(-1.0f, -1.0f));
+      acc[p][0] = fma2(tr, dx, fma2(Ar, x0r, fma2(nAi, x0i, acc[p][0])));
+      acc[p][1] = fma2(ti, dx, fma2(Ar, x0i, fma2(Ai, x0r, acc[p][1])));
+      acc[p][2] = fma2(tr, dy, fma2(Ar, x1r, fma2(nAi, x1i, acc[p][2])));
+      acc[p][3] = fma2(ti, dy, fma2(Ar, x1i, fma2(Ai, x1r, acc[p][3])));
+      acc[p][4] = fma2(tr, dz, fma2(Ar, x2r, fma2(nAi, x2i, acc[p][4])));
+      acc[p][5] = fma2(ti, dz, fma2(Ar, x2i, fma2(Ai, x2r, acc[p][5])));
+    }
+  }
+}
+
+// partial[blockIdx.y][3i + c] = sum over this split of G(r_i - r_j) x'_j
+template <bool FAST, bool IMAGE, bool LOFREE, int RP, int MINB>
+__global__ void __launch_bounds__(kOtfBlock, MINB)
+otf_pairs_f32(int n, const float4* __restrict__ obs_hi, const float4* __restrict__ obs_lo,
+              const float4* __restrict__ src_hi, const float4* __restrict__ src_lo,
+              const double2* __restrict__ x, float2 m0, float2 m1, float2 m2, float k,
+              float inv_k, float s0, int chunk, float2* __restrict__ partial,
+              const int* __restrict__ skip) {
+  if (skip && *skip) return;  // CTA-uniform: the solve no longer needs this product
+  constexpr int ROWS = 2 * RP;
+  __shared__ float4 sS[6][kOtfBlock];
+  const int tid = threadIdx.x;
+  const int row0 = blockIdx.x * (kOtfBlock * ROWS);
+  int irow[ROWS];
+  float2 OX[RP], OY[RP], OZ[RP], LX[RP], LY[RP], LZ[RP];
+  float2 acc[RP][6];
+#pragma unroll
+  for (int p = 0; p < RP; ++p) {
+    const int ia = row0 + (2 * p) * kOtfBlock + tid, ib = ia + kOtfBlock;
+    irow[2 * p] = ia;
+    irow[2 * p + 1] = ib;
+    const float4 ha = obs_hi[min(ia, n - 1)], hb = obs_hi[min(ib, n - 1)];
+    OX[p] = f2(ha.x, hb.x);
+    OY[p] = f2(ha.y, hb.y);
+    OZ[p] = f2(ha.z, hb.z);
+    if (!LOFREE) {
+      const float4 la = obs_lo[min(ia, n - 1)], lb = obs_lo[min(ib, n - 1)];
+      LX[p] = f2(la.x, lb.x);
+      LY[p] = f2(la.y, lb.y);
+      LZ[p] = f2(la.z, lb.z);
+    } else {
+      LX[p] = LY[p] = LZ[p] = f2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int c = 0; c < 6; ++c) acc[p][c] = f2(0.f, 0.f);
+  }
+  const float2 inv_k2 = f2(inv_k, inv_k), s02 = f2(s0, s0), k2 = f2(k, k);
+  const int j_begin = blockIdx.y * chunk;
+  const int j_end = min(n, j_begin + chunk);
+  const int row_end = row0 + kOtfBlock * ROWS;
+  // Software pipeline: the source of the next tile is loaded into registers
+  // before the current tile is computed, hiding its global-load latency.
+  float4 nh = make_float4(0.f, 0.f, 0.f, 0.f), nl = nh;
+  double2 na = make_double2(0.0, 0.0), nb = na, nc = na;
+  if (j_begin < j_end && tid < min(kOtfBlock, j_end - j_begin)) {
+    const int j = j_begin + tid;
+    nh = src_hi[j];
+    if (!LOFREE) nl = src_lo[j];
+    na = x[3 * j];
+    nb = x[3 * j + 1];
+    nc = x[3 * j + 2];
+  }
+  for (int jt = j_begin; jt < j_end; jt += kOtfBlock) {
+    const int cnt = min(kOtfBlock, j_end - jt);
+    __syncthreads();
+    if (tid < cnt) {
+      float2 xa = f2((float)na.x, (float)na.y), xb = f2((float)nb.x, (float)nb.y),
+             xc = f2((float)nc.x, (float)nc.y);
+      if (IMAGE) {  // x'_b = m_b x_b, m = (-r, -r, +r)  (assembly.rs:288-292)
+        xa = f2(m0.x * xa.x - m0.y * xa.y, m0.x * xa.y + m0.y * xa.x);
+        xb = f2(m1.x * xb.x - m1.y * xb.y, m1.x * xb.y + m1.y * xb.x);
+        xc = f2(m2.x * xc.x - m2.y * xc.y, m2.x * xc.y + m2.y * xc.x);
+      }
+      sS[0][tid] = make_float4(nh.x, nh.x, nh.y, nh.y);
+      sS[1][tid] = make_float4(nh.z, nh.z, xa.x, xa.x);
+      sS[2][tid] = make_float4(xa.y, xa.y, xb.x, xb.x);
+      sS[3][tid] = make_float4(xb.y, xb.y, xc.x, xc.x);
+      sS[4][tid] = make_float4(xc.y, xc.y, nl.x, nl.x);
+      sS[5][tid] = make_float4(nl.y, nl.y, nl.z, nl.z);
+    }
+    __syncthreads();
+    {
+      const int jn = jt + kOtfBlock;
+      if (jn < j_end && tid < min(kOtfBlock, j_end - jn)) {
+        const int j = jn + tid;
+        nh = src_hi[j];
+        if (!LOFREE) nl = src_lo[j];
+        na = x[3 * j];
+        nb = x[3 * j + 1];
+        nc = x[3 * j + 2];
+      }
+    }
+    const bool diag = IMAGE || (jt < row_end && jt + kOtfBlock > row0);  // CTA-uniform
+    if (diag)
+      pair_tile_f32x2<FAST, IMAGE, LOFREE, true, RP>(sS, cnt, jt, irow, OX, OY, OZ, LX, LY, LZ,
+                                                     acc, k, inv_k2, s02, k2);
+    else
+      pair_tile_f32x2<FAST, IMAGE, LOFREE, false, RP>(sS, cnt, jt, irow, OX, OY, OZ, LX, LY,
+                                                      LZ, acc, k, inv_k2, s02, k2);
+  }
+  float2* out = partial + (size_t)blockIdx.y * (3 * (size_t)n);
+#pragma unroll
+  for (int p = 0; p < RP; ++p) {
+    if (irow[2 * p] < n) {
+      const int i = irow[2 * p];
+      out[3 * i + 0] = f2(acc[p][0].x, acc[p][1].x);
+      out[3 * i + 1] = f2(acc[p][2].x, acc[p][3].x);
+      out[3 * i + 2] = f2(acc[p][4].x, acc[p][5].x);
+    }
+    if (irow[2 * p + 1] < n) {
+      const int i = irow[2 * p + 1];
+      out[3 * i + 0] = f2(acc[p][0].y, acc[p][1].y);
+      out[3 * i + 1] = f2(acc[p][2].y, acc[p][3].y);
+      out[3 * i + 2] = f2(acc[p][4].y, acc[p][5].y);
+    }
+  }
+}
+
+}  // namespace lum
