@@ -219,6 +219,7 @@ lum_status CachedOperator::assemble(const OtfOperator& g, cudaStream_t st) {
     set_error("matrix too large for device assembly");
     return LUM_ERR_INVALID;
   }
+  if (g.has_lattice && g.table_ok) return assemble_from_table(g, precision, A.p, st);
   if (precision == LUM_FP32)
     assemble_pairs<float2><<<(unsigned)blocks, threads, 0, st>>>(
         n, g.pos64.as<double4>(), g.inv_alpha.as<double2>(), g.k, g.has_lattice, g.latdev,

@@ -122,6 +122,23 @@ struct OtfOperator {
   lum_status tune_f32(cudaStream_t st);
   std::vector<double> host_pos;  // double4 host copy (image positions are built from it)
 
+  // Periodic (Ewald) operator on a dipole lattice: every displacement is
+  // d*(da, db, dc) with integer steps, so the periodic tensor is tabulated
+  // once per unique displacement (FP64, with an FP32 copy) and the matvec
+  // gathers from the table (table.cu).  Off-lattice geometries use the
+  // per-pair Ewald kernel instead.
+  int table_ok = 0;
+  double lat_d = 0.0, lat_org[3] = {0, 0, 0};
+  int tdim[3] = {0, 0, 0};   // table extent per axis: 2*(max index) + 1
+  int tsdim = 0;             // image table z extent: 2*(max z index) + 1
+  DevBuf lidx;               // int4[n] integer lattice coordinates
+  DevBuf tab64, tab32, img64, img32;
+  int nsplit_tab = 1;
+  lum_status table_detect(cudaStream_t st);        // host: lattice test + lidx upload
+  lum_status table_build(cudaStream_t st);         // per wavelength / Bloch vector
+  lum_status table_apply(int precision, const double2* x, double2* part, cudaStream_t st,
+                         const int* skip, int* nparts);
+
   lum_status build_geometry(const double* pos_host, int n, cudaStream_t st);
   lum_status set_physics(double k, const double* inv_alpha_host, int use_fcd, double cell,
                          const lum_lattice* lat, const double* kb, const lum_substrate* sub,
@@ -170,6 +187,8 @@ struct GmresWork {
 };
 
 const char* f32_variant_name(int v);  // otf.cu
+lum_status assemble_from_table(const OtfOperator& g, int precision, void* A,
+                               cudaStream_t st);  // table.cu
 
 // vector kernels (gmres.cu)
 lum_status vec_norm(const double2* v, int len, GmresWork& W, int slot, cudaStream_t st);

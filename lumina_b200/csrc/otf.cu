@@ -611,6 +611,7 @@ lum_status OtfOperator::set_physics(double k_, const double* inv_alpha_host, int
       LUM_TRY(lat_recip.alloc(sizeof(double) * rc.size()));
       LUM_TRY_CUDA(cudaMemcpyAsync(lat_real.p, re.data(), lat_real.bytes, cudaMemcpyHostToDevice, st));
       LUM_TRY_CUDA(cudaMemcpyAsync(lat_recip.p, rc.data(), lat_recip.bytes, cudaMemcpyHostToDevice, st));
+      LUM_TRY(table_detect(st));
     }
   }
   if (has_lattice && !latdev.is_2d)
@@ -657,6 +658,8 @@ lum_status OtfOperator::set_physics(double k_, const double* inv_alpha_host, int
     }
   if (first) LUM_TRY(inv_alpha.alloc(sizeof(double) * ia.size()));
   LUM_TRY_CUDA(cudaMemcpyAsync(inv_alpha.p, ia.data(), inv_alpha.bytes, cudaMemcpyHostToDevice, st));
+  // periodic tensor tables for this wavelength / Bloch vector / substrate
+  if (has_lattice && table_ok) LUM_TRY(table_build(st));
   // FCD corrections for this wavelength
   if (ell_w > 0) {
     int total = ell_w * n;
@@ -682,6 +685,7 @@ lum_status OtfOperator::set_physics(double k_, const double* inv_alpha_host, int
     int occ64 = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ64, otf_pairs_f64<false>, kOtfBlock, 0);
     nsplit64 = choose_nsplit(ntiles, ntiles, std::max(1, occ64), sms);
+    nsplit64 = std::max(nsplit64, table_ok ? nsplit_tab : 1);
     const size_t bytes = std::max(sizeof(float2) * max_parts32 * 2,
                                   sizeof(double2) * (size_t)nsplit64 * 2) * 3 * (size_t)n;
     LUM_TRY(partial.alloc(bytes));
@@ -767,8 +771,25 @@ lum_status OtfOperator::apply(int precision, const double2* x, double2* y, cudaS
   const int ntiles = (n + kOtfBlock - 1) / kOtfBlock;
   const double s0 = k * k * k / (4.0 * kPi);
   const int epi_blocks = (int)(((size_t)n * kEpiTPR + 255) / 256);
+  if (has_lattice && table_ok) {
+    // Periodic operator on a dipole lattice: gather from the FP32 or FP64 table.
+    int nparts = 1;
+    if (ev0) cudaEventRecord(ev0, st);
+    LUM_TRY(table_apply(precision, x, partial.as<double2>(), st, skip, &nparts));
+    if (ev1) cudaEventRecord(ev1, st);
+    if (precision == LUM_FP32)
+      otf_epilogue<float2, float2><<<epi_blocks, 256, 0, st>>>(
+          n, x, inv_alpha.as<double2>(), partial.as<float2>(), nparts, 0, nullptr, nullptr, y,
+          skip);
+    else
+      otf_epilogue<double2, double2><<<epi_blocks, 256, 0, st>>>(
+          n, x, inv_alpha.as<double2>(), partial.as<double2>(), nparts, 0, nullptr, nullptr, y,
+          skip);
+    LUM_CHECK_LAUNCH();
+    return LUM_OK;
+  }
   if (has_lattice) {
-    // Ewald path: FP64 pair kernel for either precision.
+    // Off-lattice periodic geometry: per-pair Ewald kernel (FP64) for either precision.
     const int ns = nsplit64;
     const int chunk = ((n + ns - 1) / ns);
     dim3 grid(ntiles, ns);
