@@ -172,6 +172,41 @@ LUM_API int lum_solve_gmres_device(lum_session* s, const void* b_dev, void* x_de
                            int max_iter, int restart, int mode, lum_solve_info* info,
                            void* stream);
 
+/* ---- batched systems ------------------------------------------------------ */
+/* No single counterpart in the reference: its callers solve independent
+ * systems (clusters, wavelengths of a sweep, polarisations) one
+ * CdaSolver::solve_dipoles call at a time (cda/mod.rs:304-389, runner.rs
+ * 134-148 runs one per rayon thread).  A batch holds K isolated systems of
+ * uneven size, each with its own positions, alpha^-1, wave number and FCD
+ * cell (no lattice, no substrate), concatenated in system order: pos is
+ * 3*sum(N_s) doubles, inv_alpha 18*sum(N_s) (row-major 3x3 complex per
+ * dipole, as lum_session_create_onthefly), k and cell K doubles.  Vectors
+ * are 3*sum(N_s) complex in the same order.  A system may hold at most
+ * 21,845 dipoles.  Duplicate a system to solve it for several right-hand
+ * sides. */
+typedef struct lum_batch lum_batch;
+LUM_API int lum_batch_create(lum_ctx* ctx, int n_systems, const int* sys_dipoles,
+                             const double* pos, const double* inv_alpha, const double* k,
+                             const double* cell, int use_fcd, lum_batch** out);
+/* y_s = A_s x_s for every system (host or device vectors). */
+LUM_API int lum_batch_matvec(lum_batch* b, int precision, const double* x, double* y);
+LUM_API int lum_batch_matvec_device(lum_batch* b, int precision, const void* x_dev, void* y_dev);
+/* GMRES of lum_solve_gmres on every system at once; info has K entries.
+ * Returns NOT_CONVERGED if any system did not converge (info says which),
+ * DEVICE on a non-finite residual. */
+LUM_API int lum_batch_solve(lum_batch* b, const double* rhs, double tol, int max_iter,
+                            int restart, int mode, double* x, lum_solve_info* info);
+LUM_API int lum_batch_solve_device(lum_batch* b, const void* rhs_dev, void* x_dev, double tol,
+                                   int max_iter, int restart, int mode, lum_solve_info* info);
+LUM_API int lum_batch_set_stream(lum_batch* b, void* stream);
+/* Launch configuration: systems, dipoles, near-list width, CTAs per system
+ * cluster, vector elements per thread, pair work-list items and persistent
+ * grid per precision. */
+LUM_API int lum_batch_info(lum_batch* b, int* n_systems, int* n_dipoles, int* ell_width,
+                           int* cluster, int* elems_per_thread, int* items32, int* grid32,
+                           int* items64, int* grid64);
+LUM_API int lum_batch_destroy(lum_batch* b);
+
 /* ---- measurement --------------------------------------------------------- */
 /* While enabled, every launch of the session's dominant matvec kernel (the
  * dense pair kernel, or the GEMV of a cached session) is bracketed by CUDA

@@ -6,7 +6,8 @@ reference's ComputeBackend / MatvecSession / CdaSolver interfaces plus the
 input types (dipoles, materials, lattices, geometry).
 """
 from . import _ffi
-from .backend import (ComputeError, ConvergenceFailure, CudaBackend, CudaSession, DeviceError,
+from .backend import (ComputeError, ConvergenceFailure, CudaBackend, CudaBatch, CudaSession,
+                      DeviceError,
                       InvalidGeometry, OutOfMemory, SolverError, Unavailable, cross_sections,
                       incident_field, invert_polarisability)
 from .lattice import LatticeSpec, SubstrateRuntime, SubstrateSpec
@@ -16,7 +17,7 @@ from .types import (CrossSections, Dipole, DipoleResponse, DipoleSet, IncidentFi
                     radiative_correction, wavenumber)
 
 __all__ = [
-    "CudaBackend", "CudaSession", "CdaSolver", "ComputeError", "Unavailable", "DeviceError",
+    "CudaBackend", "CudaSession", "CudaBatch", "CdaSolver", "ComputeError", "Unavailable", "DeviceError",
     "OutOfMemory", "SolverError", "ConvergenceFailure", "InvalidGeometry", "LatticeSpec",
     "SubstrateSpec", "SubstrateRuntime", "Dipole", "DipoleSet", "IncidentField",
     "SimulationParams", "CrossSections", "DipoleResponse", "clausius_mossotti",

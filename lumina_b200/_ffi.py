@@ -97,6 +97,17 @@ SIGNATURES = {
     "lum_measure_fma_peak": (c_int, [c_void_p, POINTER(c_double), POINTER(c_double)]),
     "lum_matvec_onthefly_noalloc": (c_int, [c_int, c_void_p, c_void_p, c_double, c_void_p,
                                             c_void_p, c_void_p]),
+    "lum_batch_create": (c_int, [c_void_p, c_int, POINTER(c_int), _dp, _dp, _dp, _dp, c_int,
+                                 POINTER(c_void_p)]),
+    "lum_batch_matvec": (c_int, [c_void_p, c_int, _dp, _dp]),
+    "lum_batch_matvec_device": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),
+    "lum_batch_solve": (c_int, [c_void_p, _dp, c_double, c_int, c_int, c_int, _dp,
+                                POINTER(LumSolveInfo)]),
+    "lum_batch_solve_device": (c_int, [c_void_p, c_void_p, c_void_p, c_double, c_int, c_int,
+                                       c_int, POINTER(LumSolveInfo)]),
+    "lum_batch_set_stream": (c_int, [c_void_p, c_void_p]),
+    "lum_batch_info": (c_int, [c_void_p] + [POINTER(c_int)] * 9),
+    "lum_batch_destroy": (c_int, [c_void_p]),
 }
 
 _lib = None

@@ -296,6 +296,100 @@ class CudaSession:
         self.close()
 
 
+class CudaBatch:
+    """K independent isolated systems solved together (lum_batch_*).
+
+    Vectors are the concatenation of the systems' 3N_s complex vectors in
+    system order; ``split`` cuts one back into per-system pieces."""
+
+    def __init__(self, handle: c_void_p, sizes, owner=None):
+        self._h = handle
+        self.sizes = [int(n) for n in sizes]
+        self.offsets = np.concatenate([[0], np.cumsum(self.sizes)]).astype(np.int64)
+        self.dim = 3 * int(self.offsets[-1])
+        self._owner = owner
+        self._lib = _ffi.load()
+
+    def split(self, v: np.ndarray):
+        v = np.asarray(v)
+        return [v[3 * self.offsets[s]:3 * self.offsets[s + 1]] for s in range(len(self.sizes))]
+
+    def matvec(self, x: np.ndarray, precision="fp64") -> np.ndarray:
+        xv = _c128(x)
+        if xv.size != self.dim:
+            raise DeviceError(f"Batch dim={self.dim}, got vector len={xv.size}")
+        y = np.empty(self.dim, np.complex128)
+        _raise(self._lib.lum_batch_matvec(self._h, _prec(precision), _dp(xv.view(np.float64)),
+                                          _dp(y.view(np.float64))), "batch matvec")
+        return y
+
+    def matvec_device(self, x_ptr: int, y_ptr: int, precision="fp64") -> None:
+        _raise(self._lib.lum_batch_matvec_device(self._h, _prec(precision), c_void_p(x_ptr),
+                                                 c_void_p(y_ptr)), "batch matvec_device")
+
+    def set_stream(self, stream: int) -> None:
+        _raise(self._lib.lum_batch_set_stream(self._h, c_void_p(stream or None)), "set_stream")
+
+    def _infos(self, arr):
+        return [arr[s].as_dict() for s in range(len(self.sizes))]
+
+    def solve(self, rhs: np.ndarray, tol: float = 1e-6, max_iter: int = 1000, restart: int = 30,
+              mode="fp64", raise_on_failure: bool = True):
+        """(x, [info per system]); x is the concatenated solution."""
+        b = _c128(rhs)
+        if b.size != self.dim:
+            raise DeviceError(f"Batch dim={self.dim}, got rhs len={b.size}")
+        x = np.zeros(self.dim, np.complex128)
+        infos = (LumSolveInfo * len(self.sizes))()
+        rc = self._lib.lum_batch_solve(self._h, _dp(b.view(np.float64)), float(tol),
+                                       int(max_iter), int(restart), _mode(mode),
+                                       _dp(x.view(np.float64)), infos)
+        d = self._infos(infos)
+        if rc == _ffi.LUM_ERR_NOT_CONVERGED:
+            if raise_on_failure:
+                worst = max(i["rel_residual"] for i in d)
+                raise ConvergenceFailure(max_iter, worst, {"systems": d})
+            return x, d
+        _raise(rc, "batch solve")
+        return x, d
+
+    def solve_device(self, b_ptr: int, x_ptr: int, tol: float, max_iter: int, restart: int = 30,
+                     mode="fp64"):
+        infos = (LumSolveInfo * len(self.sizes))()
+        rc = self._lib.lum_batch_solve_device(self._h, c_void_p(b_ptr), c_void_p(x_ptr),
+                                              float(tol), int(max_iter), int(restart),
+                                              _mode(mode), infos)
+        d = self._infos(infos)
+        if rc == _ffi.LUM_ERR_NOT_CONVERGED:
+            raise ConvergenceFailure(max_iter, max(i["rel_residual"] for i in d), {"systems": d})
+        _raise(rc, "batch solve_device")
+        return d
+
+    def info(self) -> dict:
+        vals = [c_int(0) for _ in range(9)]
+        _raise(self._lib.lum_batch_info(self._h, *[byref(v) for v in vals]), "batch info")
+        keys = ("systems", "dipoles", "ell_width", "cluster", "elems_per_thread", "items32",
+                "grid32", "items64", "grid64")
+        return {k: v.value for k, v in zip(keys, vals)}
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.lum_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
 class CudaBackend:
     """ComputeBackend on one B200 (backend.rs:62-134)."""
 
@@ -360,6 +454,31 @@ class CudaBackend:
                                                      _ref(lat), _dp(kb), _ref(sub), byref(h)),
                "create_onthefly")
         return CudaSession(h, 3 * n, "onthefly", self)
+
+    def create_batch(self, systems, use_fcd=True) -> CudaBatch:
+        """Batch of isolated systems; ``systems`` is a sequence of
+        (positions (N,3), inv_alpha (N,3,3) or 9N complex, k, cell_size)."""
+        sizes, pos, ia, ks, cells = [], [], [], [], []
+        for p, inv, k, cell in systems:
+            p = np.asarray(p, np.float64).reshape(-1, 3)
+            sizes.append(p.shape[0])
+            pos.append(p)
+            ia.append(_c128(inv, 9 * p.shape[0]))
+            ks.append(float(k))
+            cells.append(float(cell))
+        if not sizes:
+            raise InvalidGeometry("a batch needs at least one system")
+        n_arr = np.asarray(sizes, np.int32)
+        P = np.ascontiguousarray(np.concatenate(pos))
+        IA = np.ascontiguousarray(np.concatenate(ia))
+        K = np.asarray(ks, np.float64)
+        C = np.asarray(cells, np.float64)
+        h = c_void_p()
+        _raise(self._lib.lum_batch_create(self._h, len(sizes),
+                                          n_arr.ctypes.data_as(ctypes.POINTER(c_int)), _dp(P),
+                                          _dp(IA.view(np.float64)), _dp(K), _dp(C),
+                                          int(bool(use_fcd)), byref(h)), "create_batch")
+        return CudaBatch(h, sizes, self)
 
     def dense_solve(self, matrix, rhs):
         """The reference's default (backend.rs:123-133): no dense LU here;

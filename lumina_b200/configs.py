@@ -100,3 +100,103 @@ def metasurface(spacing=4.0, wavelength_nm=600.0, diameter=100.0, height=40.0, p
     sub = SubstrateRuntime(0.0, fresnel_reflection_amplitude(n_substrate ** 2, 1.0))
     inc = IncidentField((math.sin(th), 0.0, math.cos(th)), (math.cos(th), 0.0, -math.sin(th)), 1.0)
     return PeriodicWorkload(w, lat, sub, (w.k * math.sin(th), 0.0, 0.0), inc)
+
+
+# ---------------------------------------------------------------------------
+# Batched clusters
+# ---------------------------------------------------------------------------
+_M64 = (1 << 64) - 1
+
+
+class SplitMix64:
+    """Vigna's splitmix64 generator (seeded, platform-independent)."""
+
+    def __init__(self, seed: int):
+        self.state = seed & _M64
+
+    def next_u64(self) -> int:
+        self.state = (self.state + 0x9E3779B97F4A7C15) & _M64
+        z = self.state
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & _M64
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & _M64
+        return z ^ (z >> 31)
+
+    def uniform(self, lo: float, hi: float) -> float:
+        return lo + (hi - lo) * ((self.next_u64() >> 11) * (1.0 / (1 << 53)))
+
+
+@dataclass
+class Cluster:
+    positions: np.ndarray       # (N, 3)
+    alpha: np.ndarray           # (N, 3, 3) complex, anisotropic (ellipsoid route)
+    semi_axes: tuple
+    euler_deg: tuple
+    eps: complex
+
+
+@dataclass
+class BatchWorkload:
+    name: str
+    clusters: list
+    wavelength_nm: float
+    k: float
+    cell_size: float
+    polarisations: tuple        # real unit vectors, incidence along +z
+
+    def systems(self):
+        """(positions, alpha, k, cell, IncidentField) per (cluster, polarisation),
+        clusters outer."""
+        from .types import IncidentField
+        out = []
+        for c in self.clusters:
+            for pol in self.polarisations:
+                out.append((c.positions, c.alpha, self.k, self.cell_size,
+                            IncidentField((0.0, 0.0, 1.0), pol, 1.0)))
+        return out
+
+    @property
+    def n_dipoles(self):
+        return sum(c.positions.shape[0] for c in self.clusters) * len(self.polarisations)
+
+
+def batch_clusters(count=256, seed=0, spacing=1.5, wavelength_nm=600.0, n_range=(200, 5000),
+                   axes_range=(4.0, 20.0), polarisations=((1.0, 0.0, 0.0), (0.0, 1.0, 0.0))):
+    """``count`` Drude ellipsoids on a ``spacing`` lattice (splitmix64 ``seed``).
+
+    Per cluster: a target size N ~ U[n_range]; semi-axes ~ U[axes_range]
+    redrawn until, scaled to the volume N*spacing^3, all three stay inside
+    axes_range; Euler angles ~ U[0, 360) deg; Drude eps_inf ~ U[1, 10],
+    omega_p ~ U[8, 9.5] eV, gamma ~ U[0.05, 0.2] eV.  The ellipsoid is
+    discretised in its own frame on the centred lattice (discretise.rs:27-58)
+    and rotated, and every dipole gets the reference's anisotropic
+    ellipsoid tensor (scene.rs:507-517, types.rs:286-317): per-axis CM with
+    the ellipsoid's depolarisation factors, RRCM, R diag R^T."""
+    from .geometry import Ellipsoid, ellipsoid_depol_factors, rotation_zyx
+    from .materials import DrudeLorentz
+    from .types import ellipsoid_polarisability_tensor
+    rng = SplitMix64(seed)
+    k = wavenumber(wavelength_nm, 1.0)
+    vol = spacing ** 3
+    lo_a, hi_a = axes_range
+    clusters = []
+    for _ in range(count):
+        n_target = rng.uniform(*n_range)
+        v_target = n_target * vol
+        for _attempt in range(1000):
+            ax = [rng.uniform(lo_a, hi_a) for _ in range(3)]
+            scale = (3.0 * v_target / (4.0 * math.pi * ax[0] * ax[1] * ax[2])) ** (1.0 / 3.0)
+            ax = [a * scale for a in ax]
+            if all(lo_a <= a <= hi_a for a in ax):
+                break
+        euler = tuple(rng.uniform(0.0, 360.0) for _ in range(3))
+        drude = DrudeLorentz(rng.uniform(1.0, 10.0), rng.uniform(8.0, 9.5), rng.uniform(0.05, 0.2))
+        eps = drude.dielectric_function(wavelength_nm)
+        local = discretise_primitive(Ellipsoid((0.0, 0.0, 0.0), ax), spacing)
+        R = rotation_zyx(*euler)
+        pos = np.ascontiguousarray(local @ R.T)
+        L = ellipsoid_depol_factors(ax)
+        a = ellipsoid_polarisability_tensor(vol, L, eps, 1.0, k, R.ravel())
+        alpha = np.broadcast_to(a, (pos.shape[0], 3, 3)).copy()
+        clusters.append(Cluster(pos, alpha, tuple(ax), euler, eps))
+    return BatchWorkload(f"clusters{count}_seed{seed}_d{spacing:g}", clusters, wavelength_nm, k,
+                         spacing, tuple(polarisations))

@@ -186,6 +186,63 @@ struct GmresWork {
   ~GmresWork();
 };
 
+// --- batched systems (batch.cu + the batched kernels in otf.cu) ------------
+// Per-system control flags of a batched solve: `done` ends the system's
+// current restart cycle, `frozen` removes it from all further work.
+struct BatchFlags {
+  int done;
+  int frozen;
+  int jdone;
+  int bad;
+};
+
+// Device view of K systems concatenated into one dipole range [0, N): system
+// s owns dipoles [sys_off[s], sys_off[s+1]).  Vectors are 3N complex, and the
+// per-dipole arrays (positions, alpha^-1, near lists) are indexed globally.
+// FP32 positions are centred per system.
+struct BatchGeom {
+  int K = 0, N = 0;
+  int ell_w = 0;
+  int lofree = 0, fast = 1;
+  int nparts32 = 1, nparts64 = 1;      // partial slices (max splits of any system)
+  const int* sys_off = nullptr;        // [K+1]
+  const int* row_sys = nullptr;        // [N]
+  const int* sys_ns32 = nullptr;       // [K] source splits of each system (FP32 items)
+  const int* sys_ns64 = nullptr;       // [K]
+  const int* sys_chunk32 = nullptr;    // [K] sources per split (multiple of 128)
+  const int* sys_chunk64 = nullptr;    // [K]
+  const double* sys_k = nullptr;       // [K]
+  const double* sys_cell = nullptr;    // [K]
+  const double4* pos64 = nullptr;
+  const float4 *hi = nullptr, *lo = nullptr;
+  const double2* inv_alpha = nullptr;  // [9][N]
+  const int* near_j = nullptr;         // [W][N] global source indices, -1 padded
+  const double2* fcd64 = nullptr;      // [W][9][N]
+  const float2* fcd32 = nullptr;
+};
+
+// A pair-kernel work list: int4 items (system, first row, split, 0), ordered
+// by decreasing cost, consumed by a persistent grid through an atomic
+// counter (the last CTA to leave resets it, so the list can be replayed).
+struct BatchQueue {
+  DevBuf items;
+  int nitems = 0;
+  int grid = 0;
+  DevBuf counters;   // unsigned[2]: next item, CTAs finished
+};
+
+// skip_mode: 0 apply to every system, 1 skip systems whose cycle is done or
+// that are frozen, 2 skip frozen systems only.
+lum_status batch_near_fcd(BatchGeom& g, int use_fcd, DevBuf& near_j, DevBuf& fcd64,
+                          DevBuf& fcd32, cudaStream_t st);                           // otf.cu
+lum_status batch_queue(int precision, const std::vector<int>& off, int slots, BatchQueue& q,
+                       std::vector<int>& ns, std::vector<int>& chunk,
+                       cudaStream_t st);                                             // otf.cu
+lum_status batch_apply(const BatchGeom& g, int precision, const double2* x, double2* y,
+                       void* partial, BatchQueue& q, const BatchFlags* flags, int skip_mode,
+                       cudaStream_t st);                                             // otf.cu
+int batch_occupancy(const BatchGeom& g, int precision);                              // otf.cu
+
 const char* f32_variant_name(int v);  // otf.cu
 lum_status assemble_from_table(const OtfOperator& g, int precision, void* A,
                                cudaStream_t st);  // table.cu

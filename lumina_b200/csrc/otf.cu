@@ -45,21 +45,20 @@ namespace lum {
 // ---------------------------------------------------------------------------
 // FP64 dense pair kernel (same decomposition; sources as double4 + 3 double2)
 // ---------------------------------------------------------------------------
+// One CTA's work: rows [row0, row0 + 128) against sources [j_begin, j_end);
+// out is this split's slice of the partial buffer (shared with batch.cu).
 template <bool IMAGE>
-__global__ void __launch_bounds__(kOtfBlock)
-otf_pairs_f64(int n, const double4* __restrict__ pos, const double2* __restrict__ x,
-              double2 m0, double2 m1, double2 m2, double z_mirror, double k, double inv_k,
-              double s0, int chunk, double2* __restrict__ partial,
-              const int* __restrict__ skip) {
-  if (skip && *skip) return;
+__device__ __forceinline__ void pairs_f64_cta(int n, const double4* __restrict__ pos,
+                                              const double2* __restrict__ x, double2 m0,
+                                              double2 m1, double2 m2, double z_mirror, double k,
+                                              double inv_k, double s0, int row0, int j_begin,
+                                              int j_end, double2* __restrict__ out) {
   __shared__ double4 sP[kOtfBlock];
   __shared__ double2 sX[3 * kOtfBlock];
   const int tid = threadIdx.x;
-  const int i = blockIdx.x * kOtfBlock + tid;
+  const int i = row0 + tid;
   const double4 ri = pos[min(i, n - 1)];
   double acc[6] = {0, 0, 0, 0, 0, 0};
-  const int j_begin = blockIdx.y * chunk;
-  const int j_end = min(n, j_begin + chunk);
   for (int jt = j_begin; jt < j_end; jt += kOtfBlock) {
     const int cnt = min(kOtfBlock, j_end - jt);
     __syncthreads();
@@ -111,11 +110,23 @@ otf_pairs_f64(int n, const double4* __restrict__ pos, const double2* __restrict_
     }
   }
   if (i < n) {
-    double2* out = partial + (size_t)blockIdx.y * (3 * (size_t)n);
     out[3 * i + 0] = make_double2(acc[0], acc[1]);
     out[3 * i + 1] = make_double2(acc[2], acc[3]);
     out[3 * i + 2] = make_double2(acc[4], acc[5]);
   }
+}
+
+template <bool IMAGE>
+__global__ void __launch_bounds__(kOtfBlock)
+otf_pairs_f64(int n, const double4* __restrict__ pos, const double2* __restrict__ x,
+              double2 m0, double2 m1, double2 m2, double z_mirror, double k, double inv_k,
+              double s0, int chunk, double2* __restrict__ partial,
+              const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  const int j_begin = blockIdx.y * chunk;
+  pairs_f64_cta<IMAGE>(n, pos, x, m0, m1, m2, z_mirror, k, inv_k, s0, blockIdx.x * kOtfBlock,
+                       j_begin, min(n, j_begin + chunk),
+                       partial + (size_t)blockIdx.y * (3 * (size_t)n));
 }
 
 // ---------------------------------------------------------------------------
@@ -227,6 +238,9 @@ near_scan(int n, const double4* __restrict__ pos, double two_cell, int use_fcd,
   if (i < n && !FILL) count[i] = c;
 }
 
+__device__ void fcd_correction(const double4* __restrict__ pos, int i, int j, double k,
+                               double cell, double2 C[9]);
+
 // FCD correction per near pair: C = G_fcd(r_i, r_j) - G_point(r_i, r_j).
 // The 27-node rule, the r^2 < 1e-20 node skip and the weight
 // normalisation follow greens.rs:110-164.
@@ -238,6 +252,16 @@ fcd_table(int n, int ell_w, const double4* __restrict__ pos, const int* __restri
   const int w = idx / n, i = idx % n;
   const int j = near_j[(size_t)w * n + i];
   double2 C[9];
+  fcd_correction(pos, i, j, k, cell, C);
+  for (int e = 0; e < 9; ++e) {
+    fcd64[((size_t)w * 9 + e) * n + i] = C[e];
+    fcd32[((size_t)w * 9 + e) * n + i] = make_float2((float)C[e].x, (float)C[e].y);
+  }
+}
+
+// C = G_fcd(r_i, r_j) - G_point(r_i, r_j); zero when j < 0 (ELL padding).
+__device__ void fcd_correction(const double4* __restrict__ pos, int i, int j, double k,
+                               double cell, double2 C[9]) {
   for (int e = 0; e < 9; ++e) C[e] = make_double2(0.0, 0.0);
   if (j >= 0) {
     const double4 ro = pos[i], rs = pos[j];
@@ -274,10 +298,6 @@ fcd_table(int n, int ell_w, const double4* __restrict__ pos, const int* __restri
       C[e].x -= g[e].x;
       C[e].y -= g[e].y;
     }
-  }
-  for (int e = 0; e < 9; ++e) {
-    fcd64[((size_t)w * 9 + e) * n + i] = C[e];
-    fcd32[((size_t)w * 9 + e) * n + i] = make_float2((float)C[e].x, (float)C[e].y);
   }
 }
 
@@ -865,6 +885,332 @@ lum_status OtfOperator::apply(int precision, const double2* x, double2* y, cudaS
   otf_epilogue<double2, double2><<<epi_blocks, 256, 0, st>>>(
       n, x, inv_alpha.as<double2>(), part, nparts, ell_w, near_j.as<int>(),
       fcd64.as<double2>(), y, skip);
+  LUM_CHECK_LAUNCH();
+  return LUM_OK;
+}
+
+
+// ---------------------------------------------------------------------------
+// Batched systems: K independent clusters concatenated into one dipole range
+// (BatchGeom).  Each pair kernel is one persistent launch over a work list of
+// (system, row tile, source split) items ordered by decreasing cost, drawn
+// through an atomic counter so uneven cluster sizes balance across the SMs.
+// Items of systems that have converged (or whose restart cycle has ended)
+// are skipped at draw time.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool batch_skipped(const BatchFlags* flags, int s, int mode) {
+  if (mode == 0) return false;
+  const BatchFlags f = flags[s];
+  return f.frozen || (mode == 1 && f.done);
+}
+
+// Next item for the whole CTA, or -1 once the list is exhausted.  When the
+// list is exhausted the last CTA to leave resets both counters, so the same
+// launch can be replayed (CUDA graph) without a memset.
+__device__ __forceinline__ int batch_draw(unsigned* counters, int nitems, int* s_item) {
+  __syncthreads();
+  if (threadIdx.x == 0) *s_item = (int)atomicAdd(&counters[0], 1u);
+  __syncthreads();
+  const int it = *s_item;
+  if (it < nitems) return it;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&counters[1], 1u) == gridDim.x - 1) {
+      counters[0] = 0u;
+      counters[1] = 0u;
+    }
+  }
+  return -1;
+}
+
+template <bool FAST, bool LOFREE>
+__global__ void __launch_bounds__(kOtfBlock, 6)
+batch_pairs_f32(BatchGeom g, const double2* __restrict__ x, const int4* __restrict__ items,
+                int nitems, unsigned* counters, const BatchFlags* __restrict__ flags,
+                int skip_mode, float2* __restrict__ partial) {
+  __shared__ int s_item;
+  const size_t stride = 3 * (size_t)g.N;
+  const float2 one = make_float2(1.f, 0.f);
+  for (int it; (it = batch_draw(counters, nitems, &s_item)) >= 0;) {
+    const int4 item = items[it];
+    const int s = item.x;
+    if (batch_skipped(flags, s, skip_mode)) continue;  // CTA-uniform
+    const int off = g.sys_off[s], n = g.sys_off[s + 1] - off;
+    const int chunk = g.sys_chunk32[s];
+    const int j0 = item.z * chunk, j1 = min(n, j0 + chunk);
+    const double k = g.sys_k[s];
+    pairs_f32_cta<FAST, false, LOFREE, 1>(
+        n, g.hi + off, g.lo + off, g.hi + off, g.lo + off, x + 3 * (size_t)off, one, one, one,
+        (float)k, (float)(1.0 / k), (float)(k * k * k / (4.0 * kPi)), item.y, j0, j1,
+        partial + (size_t)item.z * stride + 3 * (size_t)off);
+  }
+}
+
+__global__ void __launch_bounds__(kOtfBlock)
+batch_pairs_f64(BatchGeom g, const double2* __restrict__ x, const int4* __restrict__ items,
+                int nitems, unsigned* counters, const BatchFlags* __restrict__ flags,
+                int skip_mode, double2* __restrict__ partial) {
+  __shared__ int s_item;
+  const size_t stride = 3 * (size_t)g.N;
+  const double2 one = make_double2(1.0, 0.0);
+  for (int it; (it = batch_draw(counters, nitems, &s_item)) >= 0;) {
+    const int4 item = items[it];
+    const int s = item.x;
+    if (batch_skipped(flags, s, skip_mode)) continue;  // CTA-uniform
+    const int off = g.sys_off[s], n = g.sys_off[s + 1] - off;
+    const int chunk = g.sys_chunk64[s];
+    const int j0 = item.z * chunk, j1 = min(n, j0 + chunk);
+    const double k = g.sys_k[s];
+    pairs_f64_cta<false>(n, g.pos64 + off, x + 3 * (size_t)off, one, one, one, 0.0, k, 1.0 / k,
+                         k * k * k / (4.0 * kPi), item.y, j0, j1,
+                         partial + (size_t)item.z * stride + 3 * (size_t)off);
+  }
+}
+
+// y = alpha^-1 x - sum(partials of the row's system) - sum_near C_ij x_j,
+// the epilogue above with per-system split counts and skip flags.
+template <typename TP, typename TC>
+__global__ void __launch_bounds__(256)
+batch_epilogue(BatchGeom g, const double2* __restrict__ x, const TP* __restrict__ partial,
+               const int* __restrict__ sys_ns, const TC* __restrict__ fcd,
+               const BatchFlags* __restrict__ flags, int skip_mode, double2* __restrict__ y) {
+  const int N = g.N;
+  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = min(gid / kEpiTPR, N - 1);
+  const int sub = gid % kEpiTPR;
+  const int s = g.row_sys[i];
+  const bool live = gid / kEpiTPR < N && !batch_skipped(flags, s, skip_mode);
+  const int nparts = live ? sys_ns[s] : 0;
+  const int ell_w = live ? g.ell_w : 0;
+  double gr[3] = {0, 0, 0}, gi[3] = {0, 0, 0};
+  const size_t stride = 3 * (size_t)N;
+  for (int p = sub; p < nparts; p += kEpiTPR) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      double2 v = to_d2(partial[p * stride + 3 * (size_t)i + a]);
+      gr[a] += v.x;
+      gi[a] += v.y;
+    }
+  }
+  for (int w = sub; w < ell_w; w += kEpiTPR) {
+    const int j = g.near_j[(size_t)w * N + i];
+    if (j < 0) break;  // lists are packed: the rest of this row is padding
+    double2 xj[3] = {x[3 * (size_t)j], x[3 * (size_t)j + 1], x[3 * (size_t)j + 2]};
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        double2 c = to_d2(fcd[((size_t)w * 9 + 3 * a + b) * N + i]);
+        gr[a] += c.x * xj[b].x - c.y * xj[b].y;
+        gi[a] += c.x * xj[b].y + c.y * xj[b].x;
+      }
+  }
+#pragma unroll
+  for (int o = 1; o < kEpiTPR; o <<= 1)
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      gr[a] += __shfl_xor_sync(0xffffffffu, gr[a], o);
+      gi[a] += __shfl_xor_sync(0xffffffffu, gi[a], o);
+    }
+  if (!live || sub != 0) return;
+  const double2 xi[3] = {x[3 * (size_t)i], x[3 * (size_t)i + 1], x[3 * (size_t)i + 2]};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    double sr = 0.0, si = 0.0;
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      double2 m = g.inv_alpha[(size_t)(3 * a + b) * N + i];
+      sr += m.x * xi[b].x - m.y * xi[b].y;
+      si += m.x * xi[b].y + m.y * xi[b].x;
+    }
+    y[3 * (size_t)i + a] = make_double2(sr - gr[a], si - gi[a]);
+  }
+}
+
+// Near-pair scan within each dipole's own system (same FP64 test as
+// near_scan); thread per dipole, sources read through L1 (a warp's dipoles
+// share a system, so the loads broadcast).
+template <bool FILL>
+__global__ void __launch_bounds__(256)
+batch_near_scan(BatchGeom g, int use_fcd, int* __restrict__ count, int ell_w,
+                int* __restrict__ near_j, int* __restrict__ coincident) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.N) return;
+  const int s = g.row_sys[i];
+  const int jb = g.sys_off[s], je = g.sys_off[s + 1];
+  const double two_cell = 2.0 * g.sys_cell[s];
+  const double4 ri = g.pos64[i];
+  int c = 0;
+  for (int j = jb; j < je; ++j) {
+    if (j == i) continue;
+    const double d = ref_dist(ri, g.pos64[j]);
+    if (d == 0.0) atomicOr(coincident, 1);
+    if (use_fcd && !(d > two_cell)) {
+      if (FILL && c < ell_w) near_j[(size_t)c * g.N + i] = j;
+      ++c;
+    }
+  }
+  if (!FILL) count[i] = c;
+}
+
+__global__ void __launch_bounds__(128)
+batch_fcd_table(BatchGeom g, double2* __restrict__ fcd64, float2* __restrict__ fcd32) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int N = g.N;
+  if (idx >= (size_t)N * g.ell_w) return;
+  const int w = (int)(idx / N), i = (int)(idx % N);
+  const int j = g.near_j[(size_t)w * N + i];
+  const int s = g.row_sys[i];
+  double2 C[9];
+  fcd_correction(g.pos64, i, j, g.sys_k[s], g.sys_cell[s], C);
+  for (int e = 0; e < 9; ++e) {
+    fcd64[((size_t)w * 9 + e) * N + i] = C[e];
+    fcd32[((size_t)w * 9 + e) * N + i] = make_float2((float)C[e].x, (float)C[e].y);
+  }
+}
+
+lum_status batch_near_fcd(BatchGeom& g, int use_fcd, DevBuf& near_j, DevBuf& fcd64,
+                          DevBuf& fcd32, cudaStream_t st) {
+  const int N = g.N;
+  DevBuf cnt, flag;
+  LUM_TRY(cnt.alloc(sizeof(int) * (size_t)N));
+  LUM_TRY(flag.alloc(sizeof(int)));
+  LUM_TRY_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(int), st));
+  const int blocks = (N + 255) / 256;
+  batch_near_scan<false><<<blocks, 256, 0, st>>>(g, use_fcd, cnt.as<int>(), 0, nullptr,
+                                                 flag.as<int>());
+  LUM_CHECK_LAUNCH();
+  std::vector<int> hc(N);
+  int hflag = 0;
+  LUM_TRY_CUDA(cudaMemcpyAsync(hc.data(), cnt.p, sizeof(int) * (size_t)N,
+                               cudaMemcpyDeviceToHost, st));
+  LUM_TRY_CUDA(cudaMemcpyAsync(&hflag, flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  LUM_TRY_CUDA(cudaStreamSynchronize(st));
+  if (hflag) {
+    set_error("Self-interaction: two dipoles of one system share a position");
+    return LUM_ERR_INVALID;
+  }
+  int w = 0;
+  for (int v : hc) w = std::max(w, v);
+  g.ell_w = w;
+  if (w == 0) {
+    near_j.release();
+    fcd64.release();
+    fcd32.release();
+    g.near_j = nullptr;
+    g.fcd64 = nullptr;
+    g.fcd32 = nullptr;
+    return LUM_OK;
+  }
+  LUM_TRY(near_j.alloc(sizeof(int) * (size_t)w * N));
+  LUM_TRY_CUDA(cudaMemsetAsync(near_j.p, 0xff, near_j.bytes, st));
+  batch_near_scan<true><<<blocks, 256, 0, st>>>(g, use_fcd, nullptr, w, near_j.as<int>(),
+                                                flag.as<int>());
+  LUM_CHECK_LAUNCH();
+  g.near_j = near_j.as<int>();
+  LUM_TRY(fcd64.alloc(sizeof(double2) * 9 * (size_t)w * N));
+  LUM_TRY(fcd32.alloc(sizeof(float2) * 9 * (size_t)w * N));
+  const size_t total = (size_t)w * N;
+  batch_fcd_table<<<(unsigned)((total + 127) / 128), 128, 0, st>>>(g, fcd64.as<double2>(),
+                                                                   fcd32.as<float2>());
+  LUM_CHECK_LAUNCH();
+  g.fcd64 = fcd64.as<double2>();
+  g.fcd32 = fcd32.as<float2>();
+  // the counts and flag buffers are freed on return: finish their users first
+  LUM_TRY_CUDA(cudaStreamSynchronize(st));
+  return LUM_OK;
+}
+
+int batch_occupancy(const BatchGeom& g, int precision) {
+  int occ = 1;
+  if (precision == LUM_FP32) {
+    if (g.fast && g.lofree)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_pairs_f32<true, true>, kOtfBlock, 0);
+    else if (g.fast)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_pairs_f32<true, false>, kOtfBlock, 0);
+    else if (g.lofree)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_pairs_f32<false, true>, kOtfBlock, 0);
+    else
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_pairs_f32<false, false>, kOtfBlock, 0);
+  } else {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_pairs_f64, kOtfBlock, 0);
+  }
+  return std::max(1, occ);
+}
+
+// Work list for one precision.  Rows per item: 256 (FP32) or 128 (FP64).
+// Systems are split over sources only when the row tiles alone would leave
+// the persistent grid short of four items per slot.
+lum_status batch_queue(int precision, const std::vector<int>& off, int slots, BatchQueue& q,
+                       std::vector<int>& ns, std::vector<int>& chunk, cudaStream_t st) {
+  const int K = (int)off.size() - 1;
+  const int rows = (precision == LUM_FP32) ? 2 * kOtfBlock : kOtfBlock;
+  long tiles = 0;
+  for (int s = 0; s < K; ++s) tiles += (off[s + 1] - off[s] + rows - 1) / rows;
+  const long want = 4L * slots;
+  const int split = tiles >= want ? 1 : (int)std::min<long>(8, (want + tiles - 1) / tiles);
+  ns.assign(K, 1);
+  chunk.assign(K, kOtfBlock);
+  struct It {
+    long cost;
+    int s, r, p;
+  };
+  std::vector<It> list;
+  for (int s = 0; s < K; ++s) {
+    const int n = off[s + 1] - off[s];
+    const int sp = std::max(1, std::min(split, (n + 2 * kOtfBlock - 1) / (2 * kOtfBlock)));
+    const int c = ((n + sp - 1) / sp + kOtfBlock - 1) / kOtfBlock * kOtfBlock;
+    ns[s] = (n + c - 1) / c;
+    chunk[s] = c;
+    for (int r = 0; r < n; r += rows)
+      for (int p = 0; p < ns[s]; ++p)
+        list.push_back({(long)std::min(rows, n - r) * std::min(c, n - p * c), s, r, p});
+  }
+  std::stable_sort(list.begin(), list.end(), [](const It& a, const It& b) { return a.cost > b.cost; });
+  std::vector<int4> items(list.size());
+  for (size_t t = 0; t < list.size(); ++t) items[t] = make_int4(list[t].s, list[t].r, list[t].p, 0);
+  q.nitems = (int)items.size();
+  q.grid = std::max(1, std::min(q.nitems, slots));
+  LUM_TRY(q.items.alloc(sizeof(int4) * items.size()));
+  LUM_TRY(q.counters.alloc(2 * sizeof(unsigned)));
+  LUM_TRY_CUDA(cudaMemcpyAsync(q.items.p, items.data(), q.items.bytes, cudaMemcpyHostToDevice, st));
+  LUM_TRY_CUDA(cudaMemsetAsync(q.counters.p, 0, q.counters.bytes, st));
+  LUM_TRY_CUDA(cudaStreamSynchronize(st));  // the host item list is freed on return
+  return LUM_OK;
+}
+
+lum_status batch_apply(const BatchGeom& g, int precision, const double2* x, double2* y,
+                       void* partial, BatchQueue& q, const BatchFlags* flags, int skip_mode,
+                       cudaStream_t st) {
+  const int epi_blocks = (int)(((size_t)g.N * kEpiTPR + 255) / 256);
+  const int4* items = q.items.as<int4>();
+  unsigned* cnt = q.counters.as<unsigned>();
+  if (precision == LUM_FP32) {
+    float2* part = static_cast<float2*>(partial);
+#define LUM_BATCH_F32(F, L)                                                             \
+  batch_pairs_f32<F, L><<<q.grid, kOtfBlock, 0, st>>>(g, x, items, q.nitems, cnt, flags, \
+                                                      skip_mode, part)
+    if (g.fast && g.lofree)
+      LUM_BATCH_F32(true, true);
+    else if (g.fast)
+      LUM_BATCH_F32(true, false);
+    else if (g.lofree)
+      LUM_BATCH_F32(false, true);
+    else
+      LUM_BATCH_F32(false, false);
+#undef LUM_BATCH_F32
+    LUM_CHECK_LAUNCH();
+    batch_epilogue<float2, float2><<<epi_blocks, 256, 0, st>>>(g, x, part, g.sys_ns32, g.fcd32,
+                                                               flags, skip_mode, y);
+    LUM_CHECK_LAUNCH();
+    return LUM_OK;
+  }
+  double2* part = static_cast<double2*>(partial);
+  batch_pairs_f64<<<q.grid, kOtfBlock, 0, st>>>(g, x, items, q.nitems, cnt, flags, skip_mode,
+                                                part);
+  LUM_CHECK_LAUNCH();
+  batch_epilogue<double2, double2><<<epi_blocks, 256, 0, st>>>(g, x, part, g.sys_ns64, g.fcd64,
+                                                               flags, skip_mode, y);
   LUM_CHECK_LAUNCH();
   return LUM_OK;
 }

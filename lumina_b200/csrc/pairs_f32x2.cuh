@@ -103,19 +103,19 @@ __device__ __forceinline__ void pair_tile_f32x2(
   }
 }
 
-// partial[blockIdx.y][3i + c] = sum over this split of G(r_i - r_j) x'_j
-template <bool FAST, bool IMAGE, bool LOFREE, int RP, int MINB>
-__global__ void __launch_bounds__(kOtfBlock, MINB)
-otf_pairs_f32(int n, const float4* __restrict__ obs_hi, const float4* __restrict__ obs_lo,
-              const float4* __restrict__ src_hi, const float4* __restrict__ src_lo,
-              const double2* __restrict__ x, float2 m0, float2 m1, float2 m2, float k,
-              float inv_k, float s0, int chunk, float2* __restrict__ partial,
-              const int* __restrict__ skip) {
-  if (skip && *skip) return;  // CTA-uniform: the solve no longer needs this product
+// One CTA's work: rows [row0, row0 + 256*RP) of a system of n dipoles against
+// sources [j_begin, j_end); out[3i + c] = sum_j G(r_i - r_j) x'_j for the
+// CTA's rows (out is this split's slice of the partial buffer).  Shared by
+// the single-system kernel below and the batched kernel (batch.cu).
+template <bool FAST, bool IMAGE, bool LOFREE, int RP>
+__device__ __forceinline__ void pairs_f32_cta(
+    int n, const float4* __restrict__ obs_hi, const float4* __restrict__ obs_lo,
+    const float4* __restrict__ src_hi, const float4* __restrict__ src_lo,
+    const double2* __restrict__ x, float2 m0, float2 m1, float2 m2, float k, float inv_k,
+    float s0, int row0, int j_begin, int j_end, float2* __restrict__ out) {
   constexpr int ROWS = 2 * RP;
   __shared__ float4 sS[6][kOtfBlock];
   const int tid = threadIdx.x;
-  const int row0 = blockIdx.x * (kOtfBlock * ROWS);
   int irow[ROWS];
   float2 OX[RP], OY[RP], OZ[RP], LX[RP], LY[RP], LZ[RP];
   float2 acc[RP][6];
@@ -140,8 +140,6 @@ otf_pairs_f32(int n, const float4* __restrict__ obs_hi, const float4* __restrict
     for (int c = 0; c < 6; ++c) acc[p][c] = f2(0.f, 0.f);
   }
   const float2 inv_k2 = f2(inv_k, inv_k), s02 = f2(s0, s0), k2 = f2(k, k);
-  const int j_begin = blockIdx.y * chunk;
-  const int j_end = min(n, j_begin + chunk);
   const int row_end = row0 + kOtfBlock * ROWS;
   // Software pipeline: the source of the next tile is loaded into registers
   // before the current tile is computed, hiding its global-load latency.
@@ -193,7 +191,6 @@ otf_pairs_f32(int n, const float4* __restrict__ obs_hi, const float4* __restrict
       pair_tile_f32x2<FAST, IMAGE, LOFREE, false, RP>(sS, cnt, jt, irow, OX, OY, OZ, LX, LY,
                                                       LZ, acc, k, inv_k2, s02, k2);
   }
-  float2* out = partial + (size_t)blockIdx.y * (3 * (size_t)n);
 #pragma unroll
   for (int p = 0; p < RP; ++p) {
     if (irow[2 * p] < n) {
@@ -209,6 +206,22 @@ otf_pairs_f32(int n, const float4* __restrict__ obs_hi, const float4* __restrict
       out[3 * i + 2] = f2(acc[p][4].y, acc[p][5].y);
     }
   }
+}
+
+// partial[blockIdx.y][3i + c] = sum over split blockIdx.y of G(r_i - r_j) x'_j
+template <bool FAST, bool IMAGE, bool LOFREE, int RP, int MINB>
+__global__ void __launch_bounds__(kOtfBlock, MINB)
+otf_pairs_f32(int n, const float4* __restrict__ obs_hi, const float4* __restrict__ obs_lo,
+              const float4* __restrict__ src_hi, const float4* __restrict__ src_lo,
+              const double2* __restrict__ x, float2 m0, float2 m1, float2 m2, float k,
+              float inv_k, float s0, int chunk, float2* __restrict__ partial,
+              const int* __restrict__ skip) {
+  if (skip && *skip) return;  // CTA-uniform: the solve no longer needs this product
+  const int j_begin = blockIdx.y * chunk;
+  pairs_f32_cta<FAST, IMAGE, LOFREE, RP>(n, obs_hi, obs_lo, src_hi, src_lo, x, m0, m1, m2, k,
+                                         inv_k, s0, blockIdx.x * (kOtfBlock * 2 * RP), j_begin,
+                                         min(n, j_begin + chunk),
+                                         partial + (size_t)blockIdx.y * (3 * (size_t)n));
 }
 
 }  // namespace lum
