@@ -1139,8 +1139,10 @@ int batch_occupancy(const BatchGeom& g, int precision) {
 }
 
 // Work list for one precision.  Rows per item: 256 (FP32) or 128 (FP64).
-// Systems are split over sources only when the row tiles alone would leave
-// the persistent grid short of four items per slot.
+// Every system is split into source chunks of about 512 dipoles, so that a
+// large system still spreads over many CTAs once the systems around it have
+// converged; a batch whose row tiles alone leave the persistent grid short
+// of four items per slot is split further.
 lum_status batch_queue(int precision, const std::vector<int>& off, int slots, BatchQueue& q,
                        std::vector<int>& ns, std::vector<int>& chunk, cudaStream_t st) {
   const int K = (int)off.size() - 1;
@@ -1148,7 +1150,8 @@ lum_status batch_queue(int precision, const std::vector<int>& off, int slots, Ba
   long tiles = 0;
   for (int s = 0; s < K; ++s) tiles += (off[s + 1] - off[s] + rows - 1) / rows;
   const long want = 4L * slots;
-  const int split = tiles >= want ? 1 : (int)std::min<long>(8, (want + tiles - 1) / tiles);
+  const int split = tiles >= want ? 1 : (int)std::min<long>(16, (want + tiles - 1) / tiles);
+  constexpr int kChunk = 512;
   ns.assign(K, 1);
   chunk.assign(K, kOtfBlock);
   struct It {
@@ -1158,7 +1161,8 @@ lum_status batch_queue(int precision, const std::vector<int>& off, int slots, Ba
   std::vector<It> list;
   for (int s = 0; s < K; ++s) {
     const int n = off[s + 1] - off[s];
-    const int sp = std::max(1, std::min(split, (n + 2 * kOtfBlock - 1) / (2 * kOtfBlock)));
+    const int sp = std::max(1, std::min(std::min(16, std::max(split, (n + kChunk - 1) / kChunk)),
+                                        (n + 2 * kOtfBlock - 1) / (2 * kOtfBlock)));
     const int c = ((n + sp - 1) / sp + kOtfBlock - 1) / kOtfBlock * kOtfBlock;
     ns[s] = (n + c - 1) / c;
     chunk[s] = c;
