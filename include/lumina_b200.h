@@ -207,6 +207,26 @@ LUM_API int lum_batch_info(lum_batch* b, int* n_systems, int* n_dipoles, int* el
                            int* items64, int* grid64);
 LUM_API int lum_batch_destroy(lum_batch* b);
 
+/* ---- adjoint gradients --------------------------------------------------- */
+/* No counterpart in the reference (it has no gradient code).  For an
+ * on-the-fly session without lattice or substrate: solves A p = E for the
+ * plane wave E_i = amplitude * e * exp(i k dhat . r_i) (polarisation e is 3
+ * complex = 6 doubles, so circular polarisation is allowed), then the adjoint
+ * A mu = conj(E) (A is complex symmetric), and returns
+ *   c_ext      = k/amplitude^2 * sum Im(conj(E) . p)   (cda/mod.rs:175-236),
+ *   moments    = p (3N complex; may be NULL),
+ *   grad_r     = dC_ext/dr (3N doubles, dipole-major),
+ *   grad_eps   = (dC_ext/dRe eps_i, dC_ext/dIm eps_i) per dipole (2N doubles;
+ *                may be NULL), given dinv_alpha_deps = d(alpha_i^-1)/d eps_i
+ *                per dipole (18N doubles like inv_alpha; NULL = zero).
+ * The FCD near/far switch is a step: the gradient is that of the branch each
+ * pair is on.  info_fwd / info_adj describe the two solves (may be NULL). */
+LUM_API int lum_grad_cext(lum_session* s, const double direction[3],
+                          const double polarisation[6], double amplitude,
+                          const double* dinv_alpha_deps, double tol, int max_iter, int restart,
+                          int mode, double* c_ext, double* moments, double* grad_r,
+                          double* grad_eps, lum_solve_info* info_fwd, lum_solve_info* info_adj);
+
 /* ---- measurement --------------------------------------------------------- */
 /* While enabled, every launch of the session's dominant matvec kernel (the
  * dense pair kernel, or the GEMV of a cached session) is bracketed by CUDA

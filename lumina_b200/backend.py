@@ -243,6 +243,39 @@ class CudaSession:
         _raise(rc, "solve_device")
         return d
 
+    # -- adjoint gradients ----------------------------------------------------
+    def grad_cext(self, direction, polarisation, amplitude: float = 1.0, dinv_alpha_deps=None,
+                  tol: float = 1e-8, max_iter: int = 1000, restart: int = 30, mode="fp64",
+                  want_eps: bool = True) -> dict:
+        """C_ext and its adjoint gradients for a plane wave with a (possibly
+        complex) polarisation: forward solve, adjoint solve with conj(E),
+        device gradient kernels.  Returns c_ext, grad_r (N,3), grad_eps (N,2:
+        d/dRe eps, d/dIm eps; zero without ``dinv_alpha_deps``), moments and
+        both solves' info."""
+        n = self.dim // 3
+        d = np.ascontiguousarray(np.asarray(direction, np.float64).reshape(3))
+        pol = np.asarray(polarisation, np.complex128).reshape(3)
+        pol6 = np.ascontiguousarray(np.stack([pol.real, pol.imag], axis=1).ravel())
+        dinv = None if dinv_alpha_deps is None else _c128(dinv_alpha_deps, 9 * n)
+        c_ext = c_double(0.0)
+        mom = np.zeros(3 * n, np.complex128)
+        gr = np.zeros(3 * n)
+        ge = np.zeros(2 * n) if want_eps else None
+        fi, ai = LumSolveInfo(), LumSolveInfo()
+        rc = self._lib.lum_grad_cext(self._h, _dp(d), _dp(pol6), float(amplitude),
+                                     None if dinv is None else dinv.ctypes.data, float(tol),
+                                     int(max_iter), int(restart), _mode(mode), byref(c_ext),
+                                     mom.ctypes.data, _dp(gr),
+                                     None if ge is None else ge.ctypes.data, byref(fi),
+                                     byref(ai))
+        if rc == _ffi.LUM_ERR_NOT_CONVERGED:
+            raise ConvergenceFailure(max_iter, max(fi.rel_residual, ai.rel_residual),
+                                     {"forward": fi.as_dict(), "adjoint": ai.as_dict()})
+        _raise(rc, "grad_cext")
+        return {"c_ext": c_ext.value, "grad_r": gr.reshape(n, 3),
+                "grad_eps": None if ge is None else ge.reshape(n, 2), "moments": mom,
+                "info_forward": fi.as_dict(), "info_adjoint": ai.as_dict()}
+
     # -- measurement --------------------------------------------------------
     def profile(self, enable: bool = True) -> None:
         _raise(self._lib.lum_session_profile(self._h, int(enable)), "profile")

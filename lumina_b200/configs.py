@@ -200,3 +200,43 @@ def batch_clusters(count=256, seed=0, spacing=1.5, wavelength_nm=600.0, n_range=
         clusters.append(Cluster(pos, alpha, tuple(ax), euler, eps))
     return BatchWorkload(f"clusters{count}_seed{seed}_d{spacing:g}", clusters, wavelength_nm, k,
                          spacing, tuple(polarisations))
+
+
+# ---------------------------------------------------------------------------
+# Chiral dimer (adjoint gradients)
+# ---------------------------------------------------------------------------
+@dataclass
+class DimerWorkload:
+    workload: Workload
+    eps: complex
+    lcp: tuple                  # complex polarisation (x + i y)/sqrt(2)
+    rcp: tuple                  # (x - i y)/sqrt(2)
+    direction: tuple = (0.0, 0.0, 1.0)
+
+    def dinv_alpha_deps(self):
+        """d(alpha^-1)/d eps per dipole for isotropic RRCM in vacuum:
+        alpha^-1 = 1/alpha_CM - i k^3/(6 pi) (types.rs:243-259) gives
+        -eps_m / (V (eps - eps_m)^2) on the diagonal."""
+        w = self.workload
+        v = w.cell_size ** 3
+        d = -1.0 / (v * (self.eps - 1.0) ** 2)
+        return np.broadcast_to(np.eye(3, dtype=np.complex128) * d, (w.n, 3, 3)).copy()
+
+
+def helix_dimer(spacing=1.0, wavelength_nm=650.0, pitch=40.0, radius=15.0, wire=5.0, turns=2.0,
+                gap=20.0):
+    """Two left-handed Au helices (axis z) side by side along x with ``gap`` nm
+    between their outer surfaces.  The reference's Helix primitive is
+    right-handed only (primitives.rs:126-211, v = axis x u), so each helix is
+    discretised right-handed and mirrored (x -> -x).  Au J&C, RRCM, FCD with
+    cell = spacing, vacuum."""
+    from .geometry import Helix
+    h = Helix((0.0, 0.0, 0.0), (0.0, 0.0, 1.0), radius, pitch, turns, wire)
+    one = discretise_primitive(h, spacing)
+    one = one * np.array([-1.0, 1.0, 1.0])[None, :]
+    shift = 2.0 * (radius + wire) + gap
+    pos = np.ascontiguousarray(np.concatenate([one, one + np.array([shift, 0.0, 0.0])[None, :]]))
+    w = au_workload(f"helix_dimer_p{pitch:g}_R{radius:g}_w{wire:g}_d{spacing:g}", pos, spacing,
+                    wavelength_nm)
+    s = 1.0 / math.sqrt(2.0)
+    return DimerWorkload(w, gold_eps(wavelength_nm), (s, 1j * s, 0.0), (s, -1j * s, 0.0))

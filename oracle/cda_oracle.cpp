@@ -1303,6 +1303,155 @@ void orc_wgsl_matvec_f32(int dim, const float* A, const float* x, float* y) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Adjoint gradient of C_ext (no reference counterpart: its own restatement,
+// pinned by central finite differences of orc_cross_sections in the tests).
+// p = A^-1 E and mu = A^-1 conj(E) by dense LU; the tensor derivative is
+// written in the r-hat form of greens.rs:34-71:
+//   G_ab = g (P delta_ab + Q n_a n_b),  g = e^{ikR}/(4 pi R),
+//   P = k^2 + ik/R - 1/R^2,  Q = -k^2 - 3ik/R + 3/R^2,  n = d/R,
+//   dG_ab/dd_c = n_c [g'(P delta + Q n n) + g (P' delta + Q' n n)]_ab
+//              + g Q [(delta_ac - n_a n_c) n_b + n_a (delta_bc - n_b n_c)] / R.
+// ---------------------------------------------------------------------------
+}  // extern "C"
+namespace {
+void dgreens(const double d[3], double k, C out[3][3][3]) {
+  double R = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  double n[3] = {d[0] / R, d[1] / R, d[2] / R};
+  C g = divs(cexp(cc(0.0, k * R)), 4.0 * PI * R);
+  C gp = mul(g, cc(-1.0 / R, k));
+  C P = cc(k * k - 1.0 / (R * R), k / R);
+  C Pp = cc(2.0 / (R * R * R), -k / (R * R));
+  C Q = cc(-k * k + 3.0 / (R * R), -3.0 * k / R);
+  C Qp = cc(-6.0 / (R * R * R), 3.0 * k / (R * R));
+  for (int c = 0; c < 3; ++c)
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) {
+        double dab = (a == b) ? 1.0 : 0.0, dac = (a == c) ? 1.0 : 0.0, dbc = (b == c) ? 1.0 : 0.0;
+        C t1 = add(muls(P, dab), muls(Q, n[a] * n[b]));
+        C t2 = add(muls(Pp, dab), muls(Qp, n[a] * n[b]));
+        C v = muls(add(mul(gp, t1), mul(g, t2)), n[c]);
+        double geo = ((dac - n[a] * n[c]) * n[b] + n[a] * (dbc - n[b] * n[c])) / R;
+        out[c][a][b] = add(v, muls(mul(g, Q), geo));
+      }
+}
+
+// d/dd of the tensor the forward operator uses for the pair (FCD average
+// for near pairs, greens.rs:94-167 with the same node skip).
+void dgreens_pair(const double ro[3], const double rs[3], double k, bool use_fcd, double cell,
+                  C out[3][3][3]) {
+  double dx = ro[0] - rs[0], dy = ro[1] - rs[1], dz = ro[2] - rs[2];
+  double dist = std::sqrt(dx * dx + dy * dy + dz * dz);
+  if (!use_fcd || dist > 2.0 * cell) {
+    double d[3] = {dx, dy, dz};
+    dgreens(d, k, out);
+    return;
+  }
+  const double nodes[3] = {-std::sqrt(3.0 / 5.0), 0.0, std::sqrt(3.0 / 5.0)};
+  const double weights[3] = {5.0 / 9.0, 8.0 / 9.0, 5.0 / 9.0};
+  double half_d = cell / 2.0;
+  for (int c = 0; c < 3; ++c)
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) out[c][a][b] = cc(0.0);
+  double total_w = 0.0;
+  for (int ix = 0; ix < 3; ++ix)
+    for (int iy = 0; iy < 3; ++iy)
+      for (int iz = 0; iz < 3; ++iz) {
+        double d[3] = {ro[0] - (rs[0] + half_d * nodes[ix]), ro[1] - (rs[1] + half_d * nodes[iy]),
+                       ro[2] - (rs[2] + half_d * nodes[iz])};
+        if (d[0] * d[0] + d[1] * d[1] + d[2] * d[2] < 1e-20) continue;
+        double w = weights[ix] * weights[iy] * weights[iz];
+        C t[3][3][3];
+        dgreens(d, k, t);
+        for (int c = 0; c < 3; ++c)
+          for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) out[c][a][b] = add(out[c][a][b], muls(t[c][a][b], w));
+        total_w += w;
+      }
+  if (total_w > 1e-30)
+    for (int c = 0; c < 3; ++c)
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) out[c][a][b] = divs(out[c][a][b], total_w);
+}
+}  // namespace
+extern "C" {
+
+int orc_grad_cext(int n, const double* pos, const double* alpha, double k, int use_fcd,
+                  double cell, const double* dir, const double* pol6, double amplitude,
+                  const double* dinv18, double* c_ext, double* grad_r, double* grad_eps,
+                  double* moments, int nthreads) {
+  const size_t dim = 3 * (size_t)n;
+  std::vector<double> A(2 * dim * dim);
+  int st = orc_assemble(n, pos, alpha, k, use_fcd, cell, nullptr, nullptr, nullptr, A.data(),
+                        nthreads);
+  if (st) return st;
+  std::vector<C> E(dim), Ec(dim);
+  for (int i = 0; i < n; ++i) {
+    const double* r = pos + 3 * (size_t)i;
+    double kdotr = k * (dir[0] * r[0] + dir[1] * r[1] + dir[2] * r[2]);
+    C ph = cexp(cc(0.0, kdotr));
+    for (int a = 0; a < 3; ++a) {
+      E[3 * i + a] = mul(cc(amplitude * pol6[2 * a], amplitude * pol6[2 * a + 1]), ph);
+      Ec[3 * i + a] = conj(E[3 * i + a]);
+    }
+  }
+  std::vector<C> p(dim), mu(dim);
+  st = orc_lu_solve((int)dim, A.data(), reinterpret_cast<const double*>(E.data()),
+                    reinterpret_cast<double*>(p.data()));
+  if (st) return st;
+  st = orc_lu_solve((int)dim, A.data(), reinterpret_cast<const double*>(Ec.data()),
+                    reinterpret_cast<double*>(mu.data()));
+  if (st) return st;
+  const double scale = k / (amplitude * amplitude);
+  C f = cc(0.0);
+  for (size_t q = 0; q < dim; ++q) f = add(f, mul(conj(E[q]), p[q]));
+  *c_ext = scale * f.im;
+  if (moments)
+    for (size_t q = 0; q < dim; ++q) {
+      moments[2 * q] = p[q].re;
+      moments[2 * q + 1] = p[q].im;
+    }
+  int nt = set_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nt)
+  for (int i = 0; i < n; ++i) {
+    const double* ri = pos + 3 * (size_t)i;
+    C df[3] = {cc(0.0), cc(0.0), cc(0.0)};
+    for (int j = 0; j < n; ++j) {
+      if (j == i) continue;
+      const double* rj = pos + 3 * (size_t)j;
+      C dG[3][3][3];
+      dgreens_pair(ri, rj, k, use_fcd != 0, cell, dG);
+      for (int c = 0; c < 3; ++c)
+        for (int a = 0; a < 3; ++a)
+          for (int b = 0; b < 3; ++b) {
+            df[c] = add(df[c], mul(mul(mu[3 * i + a], dG[c][a][b]), p[3 * j + b]));
+            df[c] = add(df[c], mul(mul(mu[3 * j + a], dG[c][a][b]), p[3 * i + b]));
+          }
+    }
+    C q = cc(0.0);
+    for (int a = 0; a < 3; ++a) {
+      q = add(q, mul(mu[3 * i + a], E[3 * i + a]));
+      q = sub(q, mul(conj(E[3 * i + a]), p[3 * i + a]));
+    }
+    for (int c = 0; c < 3; ++c) {
+      C inc = mul(cc(0.0, k * dir[c]), q);
+      grad_r[3 * (size_t)i + c] = scale * add(df[c], inc).im;
+    }
+    if (grad_eps) {
+      C fe = cc(0.0);
+      if (dinv18)
+        for (int a = 0; a < 3; ++a)
+          for (int b = 0; b < 3; ++b) {
+            const double* D = dinv18 + 18 * (size_t)i + 2 * (3 * a + b);
+            fe = add(fe, mul(mul(mu[3 * i + a], cc(D[0], D[1])), p[3 * i + b]));
+          }
+      grad_eps[2 * (size_t)i] = -scale * fe.im;
+      grad_eps[2 * (size_t)i + 1] = -scale * fe.re;
+    }
+  }
+  return 0;
+}
+
 int orc_max_threads(void) {
 #ifdef _OPENMP
   return omp_get_max_threads();

@@ -84,6 +84,8 @@ def _load():
         "orc_wgsl_assemble_f32": (None, [c_int, _dp, _dp, c_double, POINTER(c_float)]),
         "orc_wgsl_matvec_f32": (None, [c_int, POINTER(c_float), POINTER(c_float),
                                        POINTER(c_float)]),
+        "orc_grad_cext": (c_int, [c_int, _dp, _dp, c_double, c_int, c_double, _dp, _dp,
+                                  c_double, ctypes.c_void_p, _dp, _dp, _dp, _dp, c_int]),
         "orc_max_threads": (c_int, []),
     }
     for name, (res, args) in sig.items():
@@ -365,3 +367,28 @@ def wgsl_assemble_f32(pos, inv_alpha, k):
 
 def max_threads():
     return lib().orc_max_threads()
+
+
+def grad_cext(pos, alpha, k, use_fcd=False, cell_size=3.0, direction=(0, 0, 1),
+              polarisation=(1, 0, 0), amplitude=1.0, dinv_alpha_deps=None, nthreads=0):
+    """(C_ext, dC_ext/dr (N,3), dC_ext/d(Re,Im) eps (N,2), moments) by dense LU and
+    the oracle's own tensor-derivative restatement (no reference counterpart)."""
+    pos = _vec(pos).reshape(-1, 3)
+    n = pos.shape[0]
+    a = _alpha_arr(alpha, n)
+    pol = np.asarray(polarisation, np.complex128).reshape(3)
+    pol6 = np.ascontiguousarray(np.stack([pol.real, pol.imag], axis=1).ravel())
+    dinv = None
+    if dinv_alpha_deps is not None:
+        dinv = _alpha_arr(dinv_alpha_deps, n)
+    c_ext = c_double(0.0)
+    gr = np.zeros(3 * n)
+    ge = np.zeros(2 * n)
+    mom = np.zeros(3 * n, np.complex128)
+    st = lib().orc_grad_cext(n, _p(pos), _p(a.view(np.float64)), float(k), int(bool(use_fcd)),
+                             float(cell_size), _p(_vec(direction)), _p(pol6), float(amplitude),
+                             None if dinv is None else dinv.ctypes.data, ctypes.byref(c_ext),
+                             _p(gr), _p(ge), _p(mom.view(np.float64)), nthreads)
+    if st:
+        raise RuntimeError(f"orc_grad_cext failed ({st})")
+    return c_ext.value, gr.reshape(n, 3), ge.reshape(n, 2), mom
