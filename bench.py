@@ -55,6 +55,13 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--workload", default="cuboid",
+                   choices=["cuboid", "clusters", "dimer", "metasurface"],
+                   help="cuboid: the headline N=30k solve; clusters: 256 Drude ellipsoids x 2 "
+                        "polarisations in one batch; dimer: helix-dimer adjoint gradients; "
+                        "metasurface: periodic Ewald + substrate sweep")
+    p.add_argument("--clusters", type=int, default=256)
+    p.add_argument("--spacing", type=float, default=None)
     return p.parse_args()
 
 
@@ -209,6 +216,8 @@ def _ref_matvec_count(n):
 # ---------------------------------------------------------------- our arm
 def main():
     args = parse()
+    if args.workload != "cuboid":
+        return run_secondary(args)
     if args.impl == "reference":
         return run_reference(args)
     import torch
@@ -388,6 +397,234 @@ def _traffic_from_profiles():
     except (OSError, ValueError):
         pass
     return None
+
+
+# ---------------------------------------------------------------- secondary workloads
+# Not the headline line: the batched-cluster, adjoint-gradient and periodic
+# workloads, each printed as one JSON line of the same shape, for the record.
+def _timed(stream, fn):
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    out = fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return out, e0.elapsed_time(e1)
+
+
+def _plane_wave(pos, k, direction, pol, amplitude=1.0):
+    ph = np.exp(1j * k * (pos @ np.asarray(direction, np.float64)))
+    return (amplitude * ph[:, None] * np.asarray(pol, np.complex128)[None, :]).ravel()
+
+
+def run_secondary(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0  # single-GPU records; other ranks have nothing to do
+    if args.impl == "reference":
+        print(json.dumps({"impl": "reference", "workload": args.workload,
+                          "unavailable": "secondary workloads have no CPU reference arm; the "
+                                         "headline workload carries it"}), flush=True)
+        return 0
+    import torch
+    import lumina_b200 as lb
+    from lumina_b200 import _ffi, configs
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    bk = lb.CudaBackend(0)
+    fp32_peak, fp64_peak = bk.measure_fma_peak()
+    launches0 = _ffi.launch_count()
+    with ClockSampler(0) as clk:
+        if args.workload == "clusters":
+            line = _bench_clusters(args, bk, stream, torch, lb, configs, fp32_peak)
+        elif args.workload == "dimer":
+            line = _bench_dimer(args, bk, stream, torch, lb, configs)
+        else:
+            line = _bench_metasurface(args, bk, stream, torch, lb, configs)
+    line["gpu_launches"] = _ffi.launch_count() - launches0
+    line["clocks"] = clk.summary()
+    line.update({"n_gpus": 1, "warmup": args.warmup, "data": "synthetic", "vs_baseline": None})
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def _bench_clusters(args, bk, stream, torch, lb, configs, fp32_peak):
+    w = configs.batch_clusters(args.clusters, 0, spacing=args.spacing or 1.5)
+    systems = w.systems()
+    specs = [(p, lb.invert_polarisability(a), k, cell) for p, a, k, cell, _ in systems]
+    rhs = np.concatenate([lb.incident_field(p, k, inc) for p, _, k, _, inc in systems])
+    B = bk.create_batch(specs)
+    B.set_stream(stream.cuda_stream)
+    b_dev = torch.from_numpy(rhs).to("cuda")
+    x_dev = torch.zeros_like(b_dev)
+    tol, max_iter = args.tol, max(args.max_iter, 20000)
+    for _ in range(args.warmup):  # short solves: capture both cycle graphs
+        for mode in ("fp32_refine", "fp64"):
+            try:
+                B.solve_device(b_dev.data_ptr(), x_dev.data_ptr(), tol, 31, 30, mode)
+            except lb.ConvergenceFailure:
+                pass
+    ns = np.array(B.sizes, np.float64)
+    pairs = float(np.sum(ns * (ns - 1)))
+    mv = {}
+    xr = torch.randn(B.dim * 2, dtype=torch.float64, device="cuda")
+    yr = torch.empty_like(xr)
+    for prec in ("fp32", "fp64"):
+        B.matvec_device(xr.data_ptr(), yr.data_ptr(), prec)
+        _, ms = _timed(stream, lambda: [B.matvec_device(xr.data_ptr(), yr.data_ptr(), prec)
+                                        for _ in range(5)])
+        mv[prec] = ms / 5
+    info32, ms32 = _timed(stream, lambda: [B.solve_device(b_dev.data_ptr(), x_dev.data_ptr(), tol,
+                                                          max_iter, 30, "fp32_refine")
+                                           for _ in range(args.steps)][-1])
+    x32 = x_dev.cpu().numpy()
+    x64_dev = torch.zeros_like(b_dev)
+    info64, ms64 = _timed(stream, lambda: B.solve_device(b_dev.data_ptr(), x64_dev.data_ptr(), tol,
+                                                         max_iter, 30, "fp64"))
+    x64 = x64_dev.cpu().numpy()
+    err = 0.0
+    for s, (p, inv, k, cell) in enumerate(specs):
+        inc = systems[s][4]
+        sl = slice(3 * int(B.offsets[s]), 3 * int(B.offsets[s + 1]))
+        c32 = lb.cross_sections(p, inv, x32[sl], k, inc)[0]
+        c64 = lb.cross_sections(p, inv, x64[sl], k, inc)[0]
+        err = max(err, abs(c32 - c64) / abs(c64))
+    t0 = time.perf_counter()
+    B.solve(rhs, tol, max_iter, 30, "fp32_refine")  # e2e: host arrays in and out
+    e2e_s = time.perf_counter() - t0
+    its = [i["iterations"] for i in info32]
+    nd = w.n_dipoles
+    value = nd * args.steps / (ms32 * 1e-3)
+    info = B.info()
+    achieved = pairs * FLOPS_PER_PAIR / (mv["fp32"] * 1e-3) / 1e12
+    return {"metric": "dipole-solves/s, batched clusters (FP32+refine, C_ext rel err <=1e-6 vs "
+                      "FP64)", "value": value, "unit": UNIT, "steps": args.steps,
+            "ms_per_step": ms32 / args.steps, "higher_is_better": True, "scaling": "weak",
+            "dtype": "f32+f64", "mode": "fp32_refine",
+            "config": {"workload": f"{args.clusters} Drude ellipsoid clusters (1.5 nm lattice, "
+                                   f"anisotropic ellipsoid alpha, 600 nm) x 2 polarisations, "
+                                   f"splitmix64 seed 0", "systems": len(specs),
+                       "dipoles_total": nd, "n_min": int(ns.min()), "n_max": int(ns.max()),
+                       "tol": tol, "max_iter": max_iter, "batch": info},
+            "fp64_plain": {"value": nd / (ms64 * 1e-3), "ms_per_solve": ms64,
+                           "speedup_same_solves": ms64 / (ms32 / args.steps),
+                           "max_cext_rel_err": err},
+            "iterations": {"min": min(its), "mean": float(np.mean(its)), "max": max(its),
+                           "converged": sum(i["converged"] for i in info32)},
+            "e2e": {"value": nd / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(rhs.nbytes),
+                    "d2h_bytes_per_step": int(rhs.nbytes)},
+            "roofline": {"bound": "fp32", "kernel": "batch_pairs_f32", "achieved": achieved,
+                         "peak": fp32_peak / 1e3, "unit": "TFLOP/s",
+                         "frac": achieved / (fp32_peak / 1e3), "avg_launch_ms": mv["fp32"],
+                         "pairs_per_launch": pairs, "fp64_matvec_ms": mv["fp64"],
+                         "peak_source": "FP32 FMA-chain microbenchmark in this run; of measured"}}
+
+
+def _bench_dimer(args, bk, stream, torch, lb, configs):
+    d = configs.helix_dimer(args.spacing or 1.0)
+    w = d.workload
+    n = w.n
+    inv = lb.invert_polarisability(w.alpha)
+    dinv = d.dinv_alpha_deps()
+    tol, max_iter = args.tol, args.max_iter
+    S = bk.create_onthefly_session(w.positions, inv, w.k, True, w.cell_size)
+    S.set_stream(stream.cuda_stream)
+    bL = torch.from_numpy(_plane_wave(w.positions, w.k, d.direction, d.lcp)).to("cuda")
+    x = torch.zeros_like(bL)
+    for _ in range(args.warmup):
+        S.solve_device(bL.data_ptr(), x.data_ptr(), tol, max_iter, 30, "fp32_refine",
+                       stream.cuda_stream)
+    fwd, ms_fwd = _timed(stream, lambda: S.solve_device(bL.data_ptr(), x.data_ptr(), tol, max_iter,
+                                                        30, "fp32_refine", stream.cuda_stream))
+    res = {}
+    for name, pol in (("lcp", d.lcp), ("rcp", d.rcp)):
+        t0 = time.perf_counter()
+        res[name] = S.grad_cext(d.direction, pol, 1.0, dinv, tol=tol, max_iter=max_iter,
+                                mode="fp32_refine")
+        res[name]["ms"] = (time.perf_counter() - t0) * 1e3
+    # the reference's CD (fields.rs:236-253) from x and y linear solves
+    from lumina_b200.solver import circular_dichroism
+    from lumina_b200.types import DipoleResponse
+    mom = {}
+    for name, pol in (("x", (1.0, 0.0, 0.0)), ("y", (0.0, 1.0, 0.0))):
+        b = _plane_wave(w.positions, w.k, d.direction, pol)
+        xx, _ = S.solve(b, tol, max_iter, 30, "fp32_refine")
+        mom[name] = DipoleResponse(650.0, 1.0, xx.reshape(-1, 3), xx.reshape(-1, 3))
+    cd_ref = circular_dichroism(mom["x"], mom["y"], w.k)
+    ms_grad = res["lcp"]["ms"]
+    gL, gR = res["lcp"], res["rcp"]
+    return {"metric": "adjoint gradient cost / forward solve (dC_ext/dr, dC_ext/deps), helix "
+                      "dimer", "value": ms_grad / ms_fwd, "unit": "x forward solve",
+            "higher_is_better": False, "steps": 1, "ms_per_step": ms_grad, "scaling": "weak",
+            "dtype": "f32+f64", "mode": "fp32_refine",
+            "config": {"workload": f"two left-handed Au helices (pitch 40, R 15, wire 5 nm, 2 "
+                                   f"turns, {w.cell_size:g} nm lattice, 20 nm gap), 650 nm, "
+                                   f"LCP/RCP along +z", "n_dipoles": n, "tol": tol},
+            "forward_ms": ms_fwd, "gradient_ms_lcp": gL["ms"], "gradient_ms_rcp": gR["ms"],
+            "adjoint_overhead": (ms_grad - ms_fwd) / ms_fwd,
+            "iterations_forward": gL["info_forward"]["iterations"],
+            "iterations_adjoint": gL["info_adjoint"]["iterations"],
+            "c_ext_lcp": gL["c_ext"], "c_ext_rcp": gR["c_ext"],
+            "cd_true": gL["c_ext"] - gR["c_ext"], "cd_reference_formula": cd_ref,
+            "grad_cd_r_norm": float(np.linalg.norm(gL["grad_r"] - gR["grad_r"])),
+            "e2e": {"value": n / (ms_grad * 1e-3), "unit": "dipole-gradients/s",
+                    "h2d_bytes_per_step": n * 9 * 16, "d2h_bytes_per_step": n * (3 * 16 + 5 * 8)}}
+
+
+def _bench_metasurface(args, bk, stream, torch, lb, configs):
+    lams = [float(v) for v in (args.wavelengths if args.wavelengths != "520,650,800"
+                               else "500,700,900").split(",")]
+    spacing = args.spacing or 2.0
+    tol, max_iter = args.tol, args.max_iter
+    rows = []
+    for lam in lams:
+        pw = configs.metasurface(spacing=spacing, wavelength_nm=lam)
+        w = pw.workload
+        inv = lb.invert_polarisability(w.alpha)
+        t0 = time.perf_counter()
+        S = bk.create_onthefly_session(w.positions, inv, w.k, True, w.cell_size,
+                                       lattice=pw.lattice, k_bloch=pw.k_bloch,
+                                       substrate=pw.substrate)
+        S.set_stream(stream.cuda_stream)
+        setup_ms = (time.perf_counter() - t0) * 1e3
+        b = torch.from_numpy(lb.incident_field(w.positions, w.k, pw.incident)).to("cuda")
+        x32, x64 = torch.zeros_like(b), torch.zeros_like(b)
+        for _ in range(args.warmup):
+            try:
+                S.solve_device(b.data_ptr(), x32.data_ptr(), tol, 31, 30, "fp32_refine",
+                               stream.cuda_stream)
+            except lb.ConvergenceFailure:
+                pass
+        i32, ms32 = _timed(stream, lambda: S.solve_device(b.data_ptr(), x32.data_ptr(), tol,
+                                                          max_iter, 30, "fp32_refine",
+                                                          stream.cuda_stream))
+        i64, ms64 = _timed(stream, lambda: S.solve_device(b.data_ptr(), x64.data_ptr(), tol,
+                                                          max_iter, 30, "fp64",
+                                                          stream.cuda_stream))
+        c32 = lb.cross_sections(w.positions, inv, x32.cpu().numpy(), w.k, pw.incident)
+        c64 = lb.cross_sections(w.positions, inv, x64.cpu().numpy(), w.k, pw.incident)
+        rows.append({"wavelength_nm": lam, "n": w.n, "setup_ms": setup_ms, "ms_fp32_refine": ms32,
+                     "ms_fp64": ms64, "iterations": i32["iterations"],
+                     "cext_rel_err": abs(c32[0] - c64[0]) / abs(c64[0]),
+                     "kernel_config": S.kernel_config()})
+        S.close()
+    n = rows[0]["n"]
+    t32 = sum(r["ms_fp32_refine"] for r in rows)
+    t64 = sum(r["ms_fp64"] for r in rows)
+    return {"metric": "dipole-solves/s, periodic metasurface on a substrate (FP32+refine)",
+            "value": n * len(rows) / (t32 * 1e-3), "unit": UNIT, "higher_is_better": True,
+            "steps": len(rows), "ms_per_step": t32 / len(rows), "scaling": "weak",
+            "dtype": "f32+f64", "mode": "fp32_refine",
+            "config": {"workload": f"Au cylinder d100 h40 on a {spacing:g} nm lattice, square "
+                                   f"period 400 nm, Ewald 5/5, 10 deg incidence, n=1.45 "
+                                   f"substrate (Fresnel image)", "n_dipoles": n,
+                       "wavelengths_nm": lams, "tol": tol},
+            "fp64_plain": {"value": n * len(rows) / (t64 * 1e-3), "speedup_same_solves": t64 / t32,
+                           "max_cext_rel_err": max(r["cext_rel_err"] for r in rows)},
+            "per_wavelength": rows,
+            "e2e": None}
 
 
 if __name__ == "__main__":

@@ -227,6 +227,21 @@ LUM_API int lum_grad_cext(lum_session* s, const double direction[3],
                           int mode, double* c_ext, double* moments, double* grad_r,
                           double* grad_eps, lum_solve_info* info_fwd, lum_solve_info* info_adj);
 
+/* Several right-hand sides of one session (the nrhs argument of the proposed
+ * lum_solve_gmres; the reference solves polarisations one call at a time,
+ * cda/mod.rs:304-389).  b and x hold nrhs vectors of 3N complex back to back;
+ * info has nrhs entries.  Right-hand sides are solved two at a time in
+ * lockstep: each operator application evaluates every pair tensor once for
+ * both vectors.  Each vector's GMRES is the single-vector algorithm; a
+ * vector that converges first drops out.  The device variant runs on
+ * `stream` (NULL = the session stream) and returns without synchronising. */
+LUM_API int lum_solve_gmres_multi(lum_session* s, int nrhs, const double* b, double tol,
+                                  int max_iter, int restart, int mode, double* x,
+                                  lum_solve_info* info);
+LUM_API int lum_solve_gmres_multi_device(lum_session* s, int nrhs, const void* b_dev,
+                                         void* x_dev, double tol, int max_iter, int restart,
+                                         int mode, lum_solve_info* info, void* stream);
+
 /* ---- measurement --------------------------------------------------------- */
 /* While enabled, every launch of the session's dominant matvec kernel (the
  * dense pair kernel, or the GEMV of a cached session) is bracketed by CUDA

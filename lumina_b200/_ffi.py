@@ -108,6 +108,11 @@ SIGNATURES = {
     "lum_batch_set_stream": (c_int, [c_void_p, c_void_p]),
     "lum_batch_info": (c_int, [c_void_p] + [POINTER(c_int)] * 9),
     "lum_batch_destroy": (c_int, [c_void_p]),
+    "lum_solve_gmres_multi": (c_int, [c_void_p, c_int, _dp, c_double, c_int, c_int, c_int, _dp,
+                                      POINTER(LumSolveInfo)]),
+    "lum_solve_gmres_multi_device": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_double,
+                                             c_int, c_int, c_int, POINTER(LumSolveInfo),
+                                             c_void_p]),
     "lum_grad_cext": (c_int, [c_void_p, _dp, _dp, c_double, c_void_p, c_double, c_int, c_int,
                               c_int, _dp, c_void_p, _dp, c_void_p, POINTER(LumSolveInfo),
                               POINTER(LumSolveInfo)]),

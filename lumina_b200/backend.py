@@ -231,6 +231,39 @@ class CudaSession:
         _raise(rc, "solve")
         return x, d
 
+    def solve_multi(self, rhs, tol: float = 1e-6, max_iter: int = 1000, restart: int = 30,
+                    mode="fp64", raise_on_failure: bool = True):
+        """Several right-hand sides (rows of ``rhs``), two per operator
+        application; returns (x with the same shape, [info per rhs])."""
+        B = np.ascontiguousarray(np.asarray(rhs, np.complex128).reshape(-1, self.dim))
+        nrhs = B.shape[0]
+        X = np.zeros_like(B)
+        infos = (LumSolveInfo * nrhs)()
+        rc = self._lib.lum_solve_gmres_multi(self._h, nrhs, _dp(B.view(np.float64)), float(tol),
+                                             int(max_iter), int(restart), _mode(mode),
+                                             _dp(X.view(np.float64)), infos)
+        d = [infos[r].as_dict() for r in range(nrhs)]
+        if rc == _ffi.LUM_ERR_NOT_CONVERGED:
+            if raise_on_failure:
+                raise ConvergenceFailure(max_iter, max(i["rel_residual"] for i in d),
+                                         {"rhs": d})
+            return X, d
+        _raise(rc, "solve_multi")
+        return X, d
+
+    def solve_multi_device(self, nrhs: int, b_ptr: int, x_ptr: int, tol: float, max_iter: int,
+                           restart: int = 30, mode="fp64", stream: int = 0):
+        infos = (LumSolveInfo * nrhs)()
+        rc = self._lib.lum_solve_gmres_multi_device(self._h, int(nrhs), c_void_p(b_ptr),
+                                                    c_void_p(x_ptr), float(tol), int(max_iter),
+                                                    int(restart), _mode(mode), infos,
+                                                    c_void_p(stream or None))
+        d = [infos[r].as_dict() for r in range(nrhs)]
+        if rc == _ffi.LUM_ERR_NOT_CONVERGED:
+            raise ConvergenceFailure(max_iter, max(i["rel_residual"] for i in d), {"rhs": d})
+        _raise(rc, "solve_multi_device")
+        return d
+
     def solve_device(self, b_ptr: int, x_ptr: int, tol: float, max_iter: int, restart: int = 30,
                      mode="fp64", stream: int = 0) -> dict:
         info = LumSolveInfo()

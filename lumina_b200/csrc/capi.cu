@@ -101,6 +101,32 @@ lum_status lum_session::apply(int precision, const double2* x, double2* y, const
   return LUM_OK;
 }
 
+// Two vectors per application; profiled under precision + 2 (the two-vector
+// kernels), so the single-vector records stay comparable.
+lum_status lum_session::apply2(int precision, const double2* x, const double2* x2, double2* y,
+                               double2* y2, const int* skip, const int* skip2) {
+  if (kind != 0) {
+    LUM_TRY(apply(precision, x, y, skip));
+    return apply(precision, x2, y2, skip2);
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (profile) {
+    if (ev_used + 1 > ev_pool.size()) {
+      for (int q = 0; q < 64; ++q) {
+        EvRec r;
+        LUM_TRY_CUDA(cudaEventCreate(&r.a));
+        LUM_TRY_CUDA(cudaEventCreate(&r.b));
+        ev_pool.push_back(r);
+      }
+    }
+    EvRec& r = ev_pool[ev_used++];
+    r.precision = precision + 2;
+    e0 = r.a;
+    e1 = r.b;
+  }
+  return otf.apply2(precision, x, x2, y, y2, stream, e0, e1, skip, skip2);
+}
+
 static bool bad_ptr(const void* p, const char* what) {
   if (!p) {
     set_error("%s must not be NULL", what);
@@ -468,6 +494,61 @@ int lum_session_matmul_device(lum_session* s, const void* X, void* Y, int nrhs, 
   cudaSetDevice(s->ctx->device);
   return s->cached.apply_multi((const double2*)X, (double2*)Y, nrhs,
                                stream ? (cudaStream_t)stream : s->stream);
+}
+
+// nrhs right-hand sides of one session, two at a time in lockstep.
+int lum_solve_gmres_multi_device(lum_session* s, int nrhs, const void* b_dev, void* x_dev,
+                                 double tol, int max_iter, int restart, int mode,
+                                 lum_solve_info* info, void* stream) {
+  if (bad_ptr(s, "session") || bad_ptr(b_dev, "b") || bad_ptr(x_dev, "x")) return LUM_ERR_INVALID;
+  if (nrhs < 1 || (mode != LUM_SOLVE_FP64 && mode != LUM_SOLVE_FP32_REFINE) || !(tol > 0.0)) {
+    set_error("invalid multi-RHS solve (nrhs %d, mode %d, tol %g)", nrhs, mode, tol);
+    return LUM_ERR_INVALID;
+  }
+  cudaSetDevice(s->ctx->device);
+  cudaStream_t keep = s->stream;
+  if (stream) s->stream = (cudaStream_t)stream;
+  const double2* b = static_cast<const double2*>(b_dev);
+  double2* x = static_cast<double2*>(x_dev);
+  const size_t len = (size_t)s->dim;
+  lum_status worst = LUM_OK;
+  for (int r = 0; r < nrhs; r += 2) {
+    const int g = std::min(2, nrhs - r);
+    const double2* bb[2] = {b + r * len, b + (r + g - 1) * len};
+    double2* xx[2] = {x + r * len, x + (r + g - 1) * len};
+    lum_status st = lum_gmres_device_multi(s, g, bb, xx, tol, max_iter, restart, mode,
+                                           info ? info + r : nullptr, s->stream);
+    if (st == LUM_ERR_NOT_CONVERGED) {
+      worst = st;
+    } else if (st != LUM_OK) {
+      s->stream = keep;
+      return st;
+    }
+  }
+  s->stream = keep;
+  return worst;
+}
+
+int lum_solve_gmres_multi(lum_session* s, int nrhs, const double* b, double tol, int max_iter,
+                          int restart, int mode, double* x, lum_solve_info* info) {
+  if (bad_ptr(s, "session") || bad_ptr(b, "b") || bad_ptr(x, "x")) return LUM_ERR_INVALID;
+  if (nrhs < 1) {
+    set_error("nrhs must be positive");
+    return LUM_ERR_INVALID;
+  }
+  cudaSetDevice(s->ctx->device);
+  const size_t bytes = sizeof(double2) * (size_t)s->dim * nrhs;
+  DevBuf bd, xd;
+  LUM_TRY(bd.alloc(bytes));
+  LUM_TRY(xd.alloc(bytes));
+  LUM_TRY_CUDA(cudaMemcpyAsync(bd.p, b, bytes, cudaMemcpyHostToDevice, s->stream));
+  int st = lum_solve_gmres_multi_device(s, nrhs, bd.p, xd.p, tol, max_iter, restart, mode, info,
+                                        nullptr);
+  if (st == LUM_OK || st == LUM_ERR_NOT_CONVERGED) {
+    LUM_TRY_CUDA(cudaMemcpyAsync(x, xd.p, bytes, cudaMemcpyDeviceToHost, s->stream));
+    LUM_TRY_CUDA(cudaStreamSynchronize(s->stream));
+  }
+  return st;
 }
 
 int lum_solve_gmres_device(lum_session* s, const void* b, void* x, double tol, int max_iter,

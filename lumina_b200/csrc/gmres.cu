@@ -135,11 +135,27 @@ k_start_cycle(int len, const double2* __restrict__ r, double2* __restrict__ v0, 
   }
 }
 
+// Per-step arguments of one right-hand side.  The step kernels serve one or
+// two right-hand sides per launch (blockIdx.y selects the set), each with its
+// own reduction counter, so lockstep solves pay one launch per step kernel.
+struct MgsArgs {
+  double2* w;
+  double2* V;
+  double2* partials;
+  unsigned* counter;
+  GmresState* S;
+  double abs_tol, inner_thr;
+  int jmax;
+};
+
 // MGS projection i of column j: w -= h_{i-1,j} v_{i-1} (i>0); h_{i,j} = <v_i, w>.
 __global__ void __launch_bounds__(kVecThreads)
-k_mgs(int len, double2* __restrict__ w, const double2* __restrict__ V, int i, int j,
-      double2* partials, unsigned* counter, GmresState* S) {
-  if (S->done) return;  // grid-uniform
+k_mgs(int len, int i, int j, MgsArgs a0, MgsArgs a1) {
+  const MgsArgs a = blockIdx.y ? a1 : a0;
+  double2* __restrict__ w = a.w;
+  const double2* __restrict__ V = a.V;
+  GmresState* S = a.S;
+  if (S->done) return;  // uniform over this right-hand side's blocks
   const double2* vi = V + (size_t)i * len;
   const double2* vp = V + (size_t)(i > 0 ? i - 1 : 0) * len;
   const double2 hp = (i > 0) ? S->H[(i - 1) * kM + j] : make_double2(0.0, 0.0);
@@ -158,7 +174,7 @@ k_mgs(int len, double2* __restrict__ w, const double2* __restrict__ V, int i, in
   }
   acc = block_sum2(acc);
   double2 tot;
-  if (last_block_total(acc, partials, counter, &tot) && threadIdx.x == 0)
+  if (last_block_total(acc, a.partials, a.counter, &tot) && threadIdx.x == 0)
     S->H[i * kM + j] = tot;
 }
 
@@ -186,12 +202,18 @@ __device__ void givens(double2 a, double2 b, double* c, double2* s) {
 // The step's convergence test runs here too: |g_{j+1}| < abs_tol (the
 // reference's in-cycle test, iterative.rs:133) or, in the refinement mode,
 // below inner_thr; either ends the cycle by setting S->done, which turns the
-// kernels already queued for later steps of the cycle into no-ops.
+// kernels already queued for later steps of the cycle into no-ops.  The
+// cycle's last step (j + 1 == jmax) sets it too, so a second right-hand side
+// sharing the operator applications skips the steps this one does not take.
 __global__ void __launch_bounds__(kVecThreads)
-k_mgs_final(int len, double2* __restrict__ w, const double2* __restrict__ V, int j,
-            double2* partials, unsigned* counter, GmresState* S, double abs_tol,
-            double inner_thr) {
-  if (S->done) return;  // grid-uniform
+k_mgs_final(int len, int j, MgsArgs a0, MgsArgs a1) {
+  const MgsArgs a = blockIdx.y ? a1 : a0;
+  double2* __restrict__ w = a.w;
+  const double2* __restrict__ V = a.V;
+  GmresState* S = a.S;
+  const double abs_tol = a.abs_tol, inner_thr = a.inner_thr;
+  const int jmax = a.jmax;
+  if (S->done) return;  // uniform over this right-hand side's blocks
   const double2* vj = V + (size_t)j * len;
   const double2 hp = S->H[j * kM + j];
   double2 acc = make_double2(0.0, 0.0);
@@ -208,7 +230,7 @@ k_mgs_final(int len, double2* __restrict__ w, const double2* __restrict__ V, int
   __shared__ double s_hn;
   __shared__ double2 sH[kM + 1], sS[kM], sG[2];
   __shared__ double sC[kM];
-  if (!last_block_total(acc, partials, counter, &tot)) return;  // block-uniform
+  if (!last_block_total(acc, a.partials, a.counter, &tot)) return;  // block-uniform
   // last block: stage column j, the rotations and g[j..j+1] in shared memory
   const int t = threadIdx.x;
   if (t == 0) s_hn = sqrt(tot.x);
@@ -254,8 +276,8 @@ k_mgs_final(int len, double2* __restrict__ w, const double2* __restrict__ V, int
     if (!isfinite(gabs)) {
       S->bad = 1;
       S->done = 1;
-    } else if (gabs < abs_tol || gabs < inner_thr) {
-      S->done = 1;
+    } else if (gabs < abs_tol || gabs < inner_thr || j + 1 >= jmax) {
+      S->done = 1;  // the last step of the cycle also ends it (later kernels skip)
     }
   }
   __syncthreads();
@@ -264,8 +286,11 @@ k_mgs_final(int len, double2* __restrict__ w, const double2* __restrict__ V, int
 
 // v_{j+1} = w / h_{j+1,j}, or 0 on a lucky breakdown (iterative.rs:101-106)
 __global__ void __launch_bounds__(kVecThreads)
-k_next_basis(int len, const double2* __restrict__ w, double2* __restrict__ vnext,
-             const GmresState* S) {
+k_next_basis(int len, int j, MgsArgs a0, MgsArgs a1) {
+  const MgsArgs a = blockIdx.y ? a1 : a0;
+  const double2* __restrict__ w = a.w;
+  double2* __restrict__ vnext = a.V + (size_t)(j + 1) * len;
+  const GmresState* S = a.S;
   if (S->done) return;  // the basis beyond a finished step is never used
   const double hn = S->scal[1];
   const bool ok = hn > 1e-30;
@@ -375,117 +400,201 @@ lum_status read_scalars(GmresWork& W, cudaStream_t st) {
 
 using namespace lum;
 
-// Host driver; called from the C ABI with device vectors.
-lum_status lum_gmres_device(lum_session* s, const double2* b, double2* x, double tol,
-                            int max_iter, int restart, int mode, lum_solve_info* info,
-                            cudaStream_t st) {
-  auto t0 = std::chrono::steady_clock::now();
+// Host driver; called from the C ABI with device vectors.  One or two
+// right-hand sides: with two, both GMRES runs advance in lockstep and every
+// operator application serves both (lum_session::apply2), each run with its
+// own Krylov basis, Hessenberg matrix, convergence flag and restart count.
+// A run that has converged (or run out of iterations) drops out, and the
+// other continues with single-vector applications.
+namespace {
+struct RhsRun {
+  GmresWork* W = nullptr;
+  const double2* b = nullptr;
+  double2* x = nullptr;
+  double rhs_norm = 0.0, abs_tol = 0.0, beta = 0.0;
+  int total = 0, jmax = 0;
+  bool active = false;
+  lum_status result = LUM_OK;
   lum_solve_info loc{};
+};
+}  // namespace
+
+lum_status lum_gmres_device_multi(lum_session* s, int nrhs, const double2* const* b,
+                                  double2* const* x, double tol, int max_iter, int restart,
+                                  int mode, lum_solve_info* info, cudaStream_t st) {
+  if (nrhs < 1 || nrhs > 2) {
+    set_error("lum_gmres_device_multi takes one or two right-hand sides");
+    return LUM_ERR_INVALID;
+  }
+  auto t0 = std::chrono::steady_clock::now();
   const int len = s->dim;
   if (restart <= 0) restart = 30;
   const int m = std::min(std::min(restart, len), kMaxRestart);
-  GmresWork& W = s->gw;
-  LUM_TRY(W.ensure(len, m, st));
-  GmresState* S = W.state.as<GmresState>();
-  double2* V = W.V.as<double2>();
-  double2* w = W.w.as<double2>();
-  double2* r = W.r.as<double2>();
-  double2* tmp = W.tmp.as<double2>();
-  double2* parts = W.partials.as<double2>();
-  unsigned* cnt = W.counter.as<unsigned>();
-  const int nb = W.nblk;
   const int arnoldi_prec = (mode == LUM_SOLVE_FP32_REFINE) ? LUM_FP32 : LUM_FP64;
   const double inner_rel = 1e-5;
-
-  LUM_TRY_CUDA(cudaMemsetAsync(x, 0, sizeof(double2) * (size_t)len, st));
-  LUM_TRY(vec_norm(b, len, W, 3, st));
-  LUM_TRY(read_scalars(W, st));
-  const double rhs_norm = W.h_state->scal[3];
-  lum_status result = LUM_OK;
-  if (!std::isfinite(rhs_norm)) {
-    set_error("right-hand side is not finite");
-    return LUM_ERR_INVALID;
+  RhsRun run[2];
+  for (int r = 0; r < nrhs; ++r) {
+    RhsRun& R = run[r];
+    R.W = (r == 0) ? &s->gw : &s->gw2;
+    R.b = b[r];
+    R.x = x[r];
+    LUM_TRY(R.W->ensure(len, m, st));
+    LUM_TRY_CUDA(cudaMemsetAsync(R.x, 0, sizeof(double2) * (size_t)len, st));
+    LUM_TRY(vec_norm(R.b, len, *R.W, 3, st));
   }
-  if (rhs_norm < 1e-30) {
-    loc.converged = 1;
-    if (info) *info = loc;
-    return LUM_OK;
+  for (int r = 0; r < nrhs; ++r) LUM_TRY(read_scalars(*run[r].W, st));
+  for (int r = 0; r < nrhs; ++r) {
+    RhsRun& R = run[r];
+    R.rhs_norm = R.W->h_state->scal[3];
+    if (!std::isfinite(R.rhs_norm)) {
+      set_error("right-hand side is not finite");
+      return LUM_ERR_INVALID;
+    }
+    if (R.rhs_norm < 1e-30) {
+      R.loc.converged = 1;
+      continue;
+    }
+    R.abs_tol = tol * R.rhs_norm;
+    R.beta = R.rhs_norm;
+    // r = b - A*0 = b; beta = ||b|| (already in scal[3])
+    LUM_TRY_CUDA(cudaMemcpyAsync(R.W->r.p, R.b, sizeof(double2) * (size_t)len,
+                                 cudaMemcpyDeviceToDevice, st));
+    R.active = true;
   }
-  const double abs_tol = tol * rhs_norm;
-  // r = b - A*0 = b; beta = ||b|| (already in scal[3])
-  LUM_TRY_CUDA(cudaMemcpyAsync(r, b, sizeof(double2) * (size_t)len, cudaMemcpyDeviceToDevice, st));
-  double beta = rhs_norm;
-  int total = 0;
   for (;;) {
-    if (beta < abs_tol) {
-      loc.converged = 1;
-      break;
+    // the reference's loop head (iterative.rs:60-90): converged / out of steps
+    int act[2], na = 0;
+    for (int r = 0; r < nrhs; ++r) {
+      RhsRun& R = run[r];
+      if (!R.active) continue;
+      if (R.beta < R.abs_tol) {
+        R.loc.converged = 1;
+        R.active = false;
+      } else if (R.total >= max_iter) {
+        R.result = LUM_ERR_NOT_CONVERGED;
+        R.active = false;
+      } else {
+        act[na++] = r;
+      }
     }
-    if (total >= max_iter) {
-      result = LUM_ERR_NOT_CONVERGED;
-      break;
-    }
+    if (na == 0) break;
     // One restart cycle is enqueued whole: the device ends it early (S->done)
     // when a step meets the test, and the host reads the outcome once, after
     // the cycle's FP64 residual.  No host round trip per Arnoldi step.
-    const int jmax = std::min(m, max_iter - total);
-    const double inner_thr = (mode == LUM_SOLVE_FP32_REFINE) ? inner_rel * beta : 0.0;
-    const int* done = &S->done;
-    k_start_cycle<<<nb, kVecThreads, 0, st>>>(len, r, V, S, m);
-    LUM_CHECK_LAUNCH();
-    for (int j = 0; j < jmax; ++j) {
-      LUM_TRY(s->apply(arnoldi_prec, V + (size_t)j * len, w, done));
+    int jcyc = 0;
+    for (int q = 0; q < na; ++q) {
+      RhsRun& R = run[act[q]];
+      R.jmax = std::min(m, max_iter - R.total);
+      jcyc = std::max(jcyc, R.jmax);
+      GmresWork& W = *R.W;
+      k_start_cycle<<<W.nblk, kVecThreads, 0, st>>>(len, W.r.as<double2>(), W.V.as<double2>(),
+                                                    W.state.as<GmresState>(), m);
+      LUM_CHECK_LAUNCH();
+    }
+    for (int j = 0; j < jcyc; ++j) {
+      if (na == 2) {
+        GmresWork &A = *run[act[0]].W, &B = *run[act[1]].W;
+        LUM_TRY(s->apply2(arnoldi_prec, A.V.as<double2>() + (size_t)j * len,
+                          B.V.as<double2>() + (size_t)j * len, A.w.as<double2>(),
+                          B.w.as<double2>(), &A.state.as<GmresState>()->done,
+                          &B.state.as<GmresState>()->done));
+      } else {
+        GmresWork& A = *run[act[0]].W;
+        LUM_TRY(s->apply(arnoldi_prec, A.V.as<double2>() + (size_t)j * len, A.w.as<double2>(),
+                         &A.state.as<GmresState>()->done));
+      }
+      // one launch per step kernel for all live right-hand sides (grid.y);
+      // a run whose cycle has ended (its S->done) returns at once
+      MgsArgs ma[2];
+      for (int q = 0; q < na; ++q) {
+        RhsRun& R = run[act[q]];
+        GmresWork& W = *R.W;
+        ma[q] = MgsArgs{W.w.as<double2>(), W.V.as<double2>(), W.partials.as<double2>(),
+                        W.counter.as<unsigned>(), W.state.as<GmresState>(), R.abs_tol,
+                        (mode == LUM_SOLVE_FP32_REFINE) ? inner_rel * R.beta : 0.0, R.jmax};
+      }
+      if (na == 1) ma[1] = ma[0];
+      const dim3 grid(run[act[0]].W->nblk, na);
       for (int i = 0; i <= j; ++i) {
-        k_mgs<<<nb, kVecThreads, 0, st>>>(len, w, V, i, j, parts, cnt, S);
+        k_mgs<<<grid, kVecThreads, 0, st>>>(len, i, j, ma[0], ma[1]);
         LUM_CHECK_LAUNCH();
       }
-      k_mgs_final<<<nb, kVecThreads, 0, st>>>(len, w, V, j, parts, cnt, S, abs_tol, inner_thr);
+      k_mgs_final<<<grid, kVecThreads, 0, st>>>(len, j, ma[0], ma[1]);
       LUM_CHECK_LAUNCH();
-      k_next_basis<<<nb, kVecThreads, 0, st>>>(len, w, V + (size_t)(j + 1) * len, S);
+      k_next_basis<<<grid, kVecThreads, 0, st>>>(len, j, ma[0], ma[1]);
       LUM_CHECK_LAUNCH();
     }
-    k_backsub<<<1, kVecThreads, 0, st>>>(S);
-    LUM_CHECK_LAUNCH();
-    k_update_x<<<nb, kVecThreads, 0, st>>>(len, x, V, S);
-    LUM_CHECK_LAUNCH();
+    for (int q = 0; q < na; ++q) {
+      RhsRun& R = run[act[q]];
+      GmresWork& W = *R.W;
+      k_backsub<<<1, kVecThreads, 0, st>>>(W.state.as<GmresState>());
+      LUM_CHECK_LAUNCH();
+      k_update_x<<<W.nblk, kVecThreads, 0, st>>>(len, R.x, W.V.as<double2>(),
+                                                 W.state.as<GmresState>());
+      LUM_CHECK_LAUNCH();
+    }
     // true residual in FP64 (iterative.rs:147-151)
-    LUM_TRY(s->apply(LUM_FP64, x, tmp));
-    loc.matvecs_fp64++;
-    k_residual<<<nb, kVecThreads, 0, st>>>(len, b, tmp, r, parts, cnt, S);
-    LUM_CHECK_LAUNCH();
-    LUM_TRY(read_scalars(W, st));
-    const int steps = W.h_state->jdone;
-    total += steps;
-    if (arnoldi_prec == LUM_FP32)
-      loc.matvecs_fp32 += steps;
-    else
-      loc.matvecs_fp64 += steps;
-    if (W.h_state->bad) {
-      set_error("GMRES breakdown: non-finite residual estimate");
-      return LUM_ERR_DEVICE;
+    if (na == 2) {
+      RhsRun &A = run[act[0]], &B = run[act[1]];
+      LUM_TRY(s->apply2(LUM_FP64, A.x, B.x, A.W->tmp.as<double2>(), B.W->tmp.as<double2>(),
+                        nullptr, nullptr));
+    } else {
+      RhsRun& A = run[act[0]];
+      LUM_TRY(s->apply(LUM_FP64, A.x, A.W->tmp.as<double2>()));
     }
-    beta = W.h_state->scal[3];
-    loc.restarts++;
-    if (!std::isfinite(beta)) {
-      set_error("GMRES breakdown: non-finite residual");
-      return LUM_ERR_DEVICE;
+    for (int q = 0; q < na; ++q) {
+      RhsRun& R = run[act[q]];
+      GmresWork& W = *R.W;
+      R.loc.matvecs_fp64++;
+      k_residual<<<W.nblk, kVecThreads, 0, st>>>(len, R.b, W.tmp.as<double2>(), W.r.as<double2>(),
+                                                 W.partials.as<double2>(),
+                                                 W.counter.as<unsigned>(),
+                                                 W.state.as<GmresState>());
+      LUM_CHECK_LAUNCH();
     }
-    if (beta < abs_tol) {
-      loc.converged = 1;
-      break;
-    }
-    if (total >= max_iter) {
-      result = LUM_ERR_NOT_CONVERGED;
-      break;
+    for (int q = 0; q < na; ++q) LUM_TRY(read_scalars(*run[act[q]].W, st));
+    for (int q = 0; q < na; ++q) {
+      RhsRun& R = run[act[q]];
+      const GmresState* H = R.W->h_state;
+      const int steps = H->jdone;
+      R.total += steps;
+      if (arnoldi_prec == LUM_FP32)
+        R.loc.matvecs_fp32 += steps;
+      else
+        R.loc.matvecs_fp64 += steps;
+      if (H->bad) {
+        set_error("GMRES breakdown: non-finite residual estimate");
+        return LUM_ERR_DEVICE;
+      }
+      R.beta = H->scal[3];
+      R.loc.restarts++;
+      if (!std::isfinite(R.beta)) {
+        set_error("GMRES breakdown: non-finite residual");
+        return LUM_ERR_DEVICE;
+      }
     }
   }
-  loc.iterations = total;
-  loc.rel_residual = beta / rhs_norm;
-  loc.matvecs_reference = total + 2 * loc.restarts + (loc.restarts == 0 ? 1 : 0);
-  loc.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-  if (result == LUM_ERR_NOT_CONVERGED)
-    set_error("Solver failed to converge after %d iterations (residual: %.2e)", max_iter,
-              loc.rel_residual);
-  if (info) *info = loc;
+  const double secs =
+      std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  lum_status result = LUM_OK;
+  for (int r = 0; r < nrhs; ++r) {
+    RhsRun& R = run[r];
+    R.loc.iterations = R.total;
+    R.loc.rel_residual = R.rhs_norm > 0.0 ? R.beta / R.rhs_norm : 0.0;
+    R.loc.matvecs_reference = R.total + 2 * R.loc.restarts + (R.loc.restarts == 0 ? 1 : 0);
+    R.loc.seconds = secs;
+    if (R.result == LUM_ERR_NOT_CONVERGED) {
+      set_error("Solver failed to converge after %d iterations (residual: %.2e)", max_iter,
+                R.loc.rel_residual);
+      result = LUM_ERR_NOT_CONVERGED;
+    }
+    if (info) info[r] = R.loc;
+  }
   return result;
+}
+
+lum_status lum_gmres_device(lum_session* s, const double2* b, double2* x, double tol,
+                            int max_iter, int restart, int mode, lum_solve_info* info,
+                            cudaStream_t st) {
+  return lum_gmres_device_multi(s, 1, &b, &x, tol, max_iter, restart, mode, info, st);
 }

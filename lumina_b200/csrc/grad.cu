@@ -7,7 +7,8 @@
 //   dC_ext = k/|E0|^2 Im( dE^H p + mu^T (dE - dA p) ),   A mu = conj(E),
 // because A is complex symmetric (G(d) = G(d)^T = G(-d), alpha symmetric,
 // the FCD cell average symmetric in its two dipoles): the adjoint solve is a
-// forward solve of the same operator with the conjugate right-hand side.
+// forward solve of the same operator with the conjugate right-hand side, and
+// both run in lockstep so each operator application serves the two.
 //
 // Positions.  Row i and column i of A depend on r_i; with d = r_i - r_j and
 // G odd in its first derivative,
@@ -32,10 +33,6 @@
 
 #include <cmath>
 #include <vector>
-
-lum_status lum_gmres_device(lum_session* s, const double2* b, double2* x, double tol,
-                            int max_iter, int restart, int mode, lum_solve_info* info,
-                            cudaStream_t st);
 
 namespace lum {
 namespace {
@@ -300,15 +297,15 @@ int lum_grad_cext(lum_session* s, const double direction[3], const double polari
                                                  direction[1], direction[2], e0, e1, e2,
                                                  E.as<double2>(), Ec.as<double2>());
   LUM_CHECK_LAUNCH();
-  lum_solve_info fi{}, ai{};
-  lum_status rf = lum_gmres_device(s, E.as<double2>(), P.as<double2>(), tol, max_iter, restart,
-                                   mode, &fi, st);
-  if (info_fwd) *info_fwd = fi;
-  if (rf != LUM_OK) return rf;
-  lum_status ra = lum_gmres_device(s, Ec.as<double2>(), Mu.as<double2>(), tol, max_iter, restart,
-                                   mode, &ai, st);
-  if (info_adj) *info_adj = ai;
-  if (ra != LUM_OK) return ra;
+  // forward and adjoint solves in lockstep: every operator application
+  // serves both right-hand sides
+  lum_solve_info inf[2] = {};
+  const double2* bb[2] = {E.as<double2>(), Ec.as<double2>()};
+  double2* xx[2] = {P.as<double2>(), Mu.as<double2>()};
+  lum_status rs = lum_gmres_device_multi(s, 2, bb, xx, tol, max_iter, restart, mode, inf, st);
+  if (info_fwd) *info_fwd = inf[0];
+  if (info_adj) *info_adj = inf[1];
+  if (rs != LUM_OK) return rs;
   // pair pass: split the sources until the grid covers the SMs twice
   const int tiles = (n + kGradBlock - 1) / kGradBlock;
   const int sms = s->ctx->sms > 0 ? s->ctx->sms : 148;

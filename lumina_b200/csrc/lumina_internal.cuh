@@ -147,6 +147,17 @@ struct OtfOperator {
   // kernel of this application returns at once (y is left untouched).
   lum_status apply(int precision, const double2* x, double2* y, cudaStream_t st,
                    cudaEvent_t ev0, cudaEvent_t ev1, const int* skip = nullptr);
+
+  // Two right-hand sides at once (y = A x, y2 = A x2) with one skip flag
+  // each: the dense pair kernels evaluate each tensor once for both vectors.
+  DevBuf partial2;             // partial sums of the second vector
+  int f32x2_variant = -1;      // tuned two-vector FP32 variant (-1: not yet tuned)
+  int nsplit_x2 = 1;
+  float tuned_x2_ms = 0.f;
+  lum_status tune_f32_x2(cudaStream_t st);
+  lum_status apply2(int precision, const double2* x, const double2* x2, double2* y, double2* y2,
+                    cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1, const int* skip,
+                    const int* skip2);
 };
 
 // --- cached (dense matrix) operator ----------------------------------------
@@ -281,4 +292,16 @@ struct lum_session {
   std::vector<EvRec> ev_pool;
   size_t ev_used = 0;
   lum_status apply(int precision, const double2* x, double2* y, const int* skip = nullptr);
+  lum_status apply2(int precision, const double2* x, const double2* x2, double2* y, double2* y2,
+                    const int* skip, const int* skip2);
+  lum::GmresWork gw2;           // workspace of the second right-hand side
 };
+
+// Device GMRES drivers (gmres.cu): one right-hand side, or one or two in
+// lockstep sharing every operator application.
+lum_status lum_gmres_device(lum_session* s, const double2* b, double2* x, double tol,
+                            int max_iter, int restart, int mode, lum_solve_info* info,
+                            cudaStream_t st);
+lum_status lum_gmres_device_multi(lum_session* s, int nrhs, const double2* const* b,
+                                  double2* const* x, double tol, int max_iter, int restart,
+                                  int mode, lum_solve_info* info, cudaStream_t st);

@@ -46,19 +46,23 @@ namespace lum {
 // FP64 dense pair kernel (same decomposition; sources as double4 + 3 double2)
 // ---------------------------------------------------------------------------
 // One CTA's work: rows [row0, row0 + 128) against sources [j_begin, j_end);
-// out is this split's slice of the partial buffer (shared with batch.cu).
-template <bool IMAGE>
+// out is this split's slice of the partial buffer (shared with the batched
+// kernel).  NR == 2 also contracts the same tensors with x2 into out2.
+template <bool IMAGE, int NR>
 __device__ __forceinline__ void pairs_f64_cta(int n, const double4* __restrict__ pos,
-                                              const double2* __restrict__ x, double2 m0,
+                                              const double2* __restrict__ x,
+                                              const double2* __restrict__ x2, double2 m0,
                                               double2 m1, double2 m2, double z_mirror, double k,
                                               double inv_k, double s0, int row0, int j_begin,
-                                              int j_end, double2* __restrict__ out) {
+                                              int j_end, double2* __restrict__ out,
+                                              double2* __restrict__ out2) {
   __shared__ double4 sP[kOtfBlock];
-  __shared__ double2 sX[3 * kOtfBlock];
+  __shared__ double2 sX[3 * NR * kOtfBlock];
   const int tid = threadIdx.x;
   const int i = row0 + tid;
   const double4 ri = pos[min(i, n - 1)];
   double acc[6] = {0, 0, 0, 0, 0, 0};
+  double acc2[6] = {0, 0, 0, 0, 0, 0};
   for (int jt = j_begin; jt < j_end; jt += kOtfBlock) {
     const int cnt = min(kOtfBlock, j_end - jt);
     __syncthreads();
@@ -76,6 +80,17 @@ __device__ __forceinline__ void pairs_f64_cta(int n, const double4* __restrict__
       sX[3 * tid] = a;
       sX[3 * tid + 1] = b;
       sX[3 * tid + 2] = c;
+      if constexpr (NR == 2) {
+        double2 d = x2[3 * j], e = x2[3 * j + 1], f = x2[3 * j + 2];
+        if (IMAGE) {
+          d = make_double2(m0.x * d.x - m0.y * d.y, m0.x * d.y + m0.y * d.x);
+          e = make_double2(m1.x * e.x - m1.y * e.y, m1.x * e.y + m1.y * e.x);
+          f = make_double2(m2.x * f.x - m2.y * f.y, m2.x * f.y + m2.y * f.x);
+        }
+        sX[3 * kOtfBlock + 3 * tid] = d;
+        sX[3 * kOtfBlock + 3 * tid + 1] = e;
+        sX[3 * kOtfBlock + 3 * tid + 2] = f;
+      }
     }
     __syncthreads();
     for (int jj = 0; jj < cnt; ++jj) {
@@ -107,12 +122,30 @@ __device__ __forceinline__ void pairs_f64_cta(int n, const double4* __restrict__
       acc[3] += Ar * xb.y + Ai * xb.x + ti * dy;
       acc[4] += Ar * xc.x - Ai * xc.y + tr * dz;
       acc[5] += Ar * xc.y + Ai * xc.x + ti * dz;
+      if constexpr (NR == 2) {
+        const double2 ya = sX[3 * kOtfBlock + 3 * jj], yb = sX[3 * kOtfBlock + 3 * jj + 1],
+                      yc = sX[3 * kOtfBlock + 3 * jj + 2];
+        double dyr = dx * ya.x + dy * yb.x + dz * yc.x;
+        double dyi = dx * ya.y + dy * yb.y + dz * yc.y;
+        double ur = Br * dyr - Bi * dyi, ui = Br * dyi + Bi * dyr;
+        acc2[0] += Ar * ya.x - Ai * ya.y + ur * dx;
+        acc2[1] += Ar * ya.y + Ai * ya.x + ui * dx;
+        acc2[2] += Ar * yb.x - Ai * yb.y + ur * dy;
+        acc2[3] += Ar * yb.y + Ai * yb.x + ui * dy;
+        acc2[4] += Ar * yc.x - Ai * yc.y + ur * dz;
+        acc2[5] += Ar * yc.y + Ai * yc.x + ui * dz;
+      }
     }
   }
   if (i < n) {
     out[3 * i + 0] = make_double2(acc[0], acc[1]);
     out[3 * i + 1] = make_double2(acc[2], acc[3]);
     out[3 * i + 2] = make_double2(acc[4], acc[5]);
+    if constexpr (NR == 2) {
+      out2[3 * i + 0] = make_double2(acc2[0], acc2[1]);
+      out2[3 * i + 1] = make_double2(acc2[2], acc2[3]);
+      out2[3 * i + 2] = make_double2(acc2[4], acc2[5]);
+    }
   }
 }
 
@@ -124,9 +157,31 @@ otf_pairs_f64(int n, const double4* __restrict__ pos, const double2* __restrict_
               const int* __restrict__ skip) {
   if (skip && *skip) return;
   const int j_begin = blockIdx.y * chunk;
-  pairs_f64_cta<IMAGE>(n, pos, x, m0, m1, m2, z_mirror, k, inv_k, s0, blockIdx.x * kOtfBlock,
-                       j_begin, min(n, j_begin + chunk),
-                       partial + (size_t)blockIdx.y * (3 * (size_t)n));
+  pairs_f64_cta<IMAGE, 1>(n, pos, x, nullptr, m0, m1, m2, z_mirror, k, inv_k, s0,
+                          blockIdx.x * kOtfBlock, j_begin, min(n, j_begin + chunk),
+                          partial + (size_t)blockIdx.y * (3 * (size_t)n), nullptr);
+}
+
+// Two right-hand sides (see otf_pairs_f32_x2).
+template <bool IMAGE>
+__global__ void __launch_bounds__(kOtfBlock)
+otf_pairs_f64_x2(int n, const double4* __restrict__ pos, const double2* __restrict__ x,
+                 const double2* __restrict__ x2, double2 m0, double2 m1, double2 m2,
+                 double z_mirror, double k, double inv_k, double s0, int chunk,
+                 double2* __restrict__ partial, double2* __restrict__ partial2,
+                 const int* __restrict__ skip, const int* __restrict__ skip2) {
+  const bool live = !(skip && *skip), live2 = !(skip2 && *skip2);
+  if (!live && !live2) return;
+  const int j_begin = blockIdx.y * chunk, j_end = min(n, j_begin + chunk);
+  const size_t off = (size_t)blockIdx.y * (3 * (size_t)n);
+  if (live && live2)
+    pairs_f64_cta<IMAGE, 2>(n, pos, x, x2, m0, m1, m2, z_mirror, k, inv_k, s0,
+                            blockIdx.x * kOtfBlock, j_begin, j_end, partial + off,
+                            partial2 + off);
+  else
+    pairs_f64_cta<IMAGE, 1>(n, pos, live ? x : x2, nullptr, m0, m1, m2, z_mirror, k, inv_k, s0,
+                            blockIdx.x * kOtfBlock, j_begin, j_end,
+                            (live ? partial : partial2) + off, nullptr);
 }
 
 // ---------------------------------------------------------------------------
@@ -445,6 +500,66 @@ const F32VariantEntry kF32Variants[] = {
 };
 constexpr int kNumF32Variants = sizeof(kF32Variants) / sizeof(kF32Variants[0]);
 
+// Two-vector variants (otf_pairs_f32_x2): the second accumulator set needs
+// more registers, so the register caps are looser.
+struct F32X2Args {
+  int n;
+  const float4 *oh, *ol, *sh, *sl;
+  const double2 *x, *x2;
+  float2 m0, m1, m2;
+  float k, ik, s0;
+  int chunk;
+  float2 *part, *part2;
+  const int *skip, *skip2;
+};
+
+template <int RP, int MINB>
+struct F32X2Variant {
+  template <bool IMAGE>
+  static void launch(int fast, int lofree, dim3 grid, cudaStream_t st, const F32X2Args& a) {
+#define LUM_F32X2_LAUNCH(F, L)                                                                \
+  otf_pairs_f32_x2<F, IMAGE, L, RP, MINB><<<grid, kOtfBlock, 0, st>>>(                         \
+      a.n, a.oh, a.ol, a.sh, a.sl, a.x, a.x2, a.m0, a.m1, a.m2, a.k, a.ik, a.s0, a.chunk,      \
+      a.part, a.part2, a.skip, a.skip2)
+    if (fast && lofree)
+      LUM_F32X2_LAUNCH(true, true);
+    else if (fast)
+      LUM_F32X2_LAUNCH(true, false);
+    else if (lofree)
+      LUM_F32X2_LAUNCH(false, true);
+    else
+      LUM_F32X2_LAUNCH(false, false);
+#undef LUM_F32X2_LAUNCH
+  }
+  static int occupancy(int fast, int lofree) {
+    int occ = 1;
+    if (fast && lofree)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, otf_pairs_f32_x2<true, false, true, RP, MINB>, kOtfBlock, 0);
+    else if (fast)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, otf_pairs_f32_x2<true, false, false, RP, MINB>, kOtfBlock, 0);
+    else if (lofree)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, otf_pairs_f32_x2<false, false, true, RP, MINB>, kOtfBlock, 0);
+    else
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, otf_pairs_f32_x2<false, false, false, RP, MINB>, kOtfBlock, 0);
+    return std::max(1, occ);
+  }
+};
+
+struct F32X2VariantEntry {
+  const char* name;
+  int rows;
+  void (*direct)(int, int, dim3, cudaStream_t, const F32X2Args&);
+  void (*image)(int, int, dim3, cudaStream_t, const F32X2Args&);
+  int (*occupancy)(int, int);
+};
+
+const F32X2VariantEntry kF32X2Variants[] = {
+    {"x2_rows2_minb4", 2, F32X2Variant<1, 4>::launch<false>, F32X2Variant<1, 4>::launch<true>, F32X2Variant<1, 4>::occupancy},
+    {"x2_rows4_minb2", 4, F32X2Variant<2, 2>::launch<false>, F32X2Variant<2, 2>::launch<true>, F32X2Variant<2, 2>::occupancy},
+};
+constexpr int kNumF32X2Variants = sizeof(kF32X2Variants) / sizeof(kF32X2Variants[0]);
+std::map<std::tuple<int, int, int>, int> g_tune_x2_cache;
+
 }  // namespace
 
 const char* f32_variant_name(int v) {
@@ -710,7 +825,10 @@ lum_status OtfOperator::set_physics(double k_, const double* inv_alpha_host, int
                                   sizeof(double2) * (size_t)nsplit64 * 2) * 3 * (size_t)n;
     LUM_TRY(partial.alloc(bytes));
   }
-  if (first || old_fast != fast_trig) LUM_TRY(tune_f32(st));
+  if (first || old_fast != fast_trig) {
+    LUM_TRY(tune_f32(st));
+    f32x2_variant = -1;  // the two-vector variant is tuned again on first use
+  }
   return LUM_OK;
 }
 
@@ -891,6 +1009,165 @@ lum_status OtfOperator::apply(int precision, const double2* x, double2* y, cudaS
 
 
 // ---------------------------------------------------------------------------
+// Two right-hand sides per application (multi-RHS solves, forward + adjoint)
+// ---------------------------------------------------------------------------
+lum_status OtfOperator::tune_f32_x2(cudaStream_t st) {
+  const int sms = device_sms();
+  const int ntiles = (n + kOtfBlock - 1) / kOtfBlock;
+  // room for the direct and image splits of each vector in partial / partial2
+  const int cap = std::max(1, (int)(partial.bytes / (sizeof(float2) * 3 * (size_t)n * 2)));
+  int ns_v[kNumF32X2Variants];
+  for (int v = 0; v < kNumF32X2Variants; ++v) {
+    const int rows = kF32X2Variants[v].rows;
+    const int rb = (n + kOtfBlock * rows - 1) / (kOtfBlock * rows);
+    ns_v[v] = std::min(cap, choose_nsplit(rb, ntiles, kF32X2Variants[v].occupancy(fast_trig, lofree),
+                                          sms));
+  }
+  f32x2_variant = 0;
+  const char* env = std::getenv("LUMINA_TUNE");
+  const auto key = std::make_tuple(n, fast_trig, lofree);
+  if ((env && env[0] == '0') || n < 2048) {
+    nsplit_x2 = ns_v[0];
+    return LUM_OK;
+  }
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_x2_cache.find(key);
+    if (it != g_tune_x2_cache.end()) {
+      f32x2_variant = it->second;
+      nsplit_x2 = ns_v[f32x2_variant];
+      return LUM_OK;
+    }
+  }
+  DevBuf xz;
+  LUM_TRY(xz.alloc(sizeof(double2) * 3 * (size_t)n));
+  LUM_TRY_CUDA(cudaMemsetAsync(xz.p, 0, xz.bytes, st));
+  cudaEvent_t e0, e1;
+  LUM_TRY_CUDA(cudaEventCreate(&e0));
+  LUM_TRY_CUDA(cudaEventCreate(&e1));
+  const double s0 = k * k * k / (4.0 * kPi);
+  float best = 1e30f;
+  for (int v = 0; v < kNumF32X2Variants; ++v) {
+    const int rows = kF32X2Variants[v].rows, ns = ns_v[v];
+    const int chunk = ((ntiles + ns - 1) / ns) * kOtfBlock;
+    dim3 grid((n + kOtfBlock * rows - 1) / (kOtfBlock * rows), ns);
+    const float2 one = make_float2(1.f, 0.f);
+    F32X2Args a{n, pos_hi.as<float4>(), pos_lo.as<float4>(), pos_hi.as<float4>(),
+                pos_lo.as<float4>(), xz.as<double2>(), xz.as<double2>(), one, one, one,
+                (float)k, (float)(1.0 / k), (float)s0, chunk, partial.as<float2>(),
+                partial2.as<float2>(), nullptr, nullptr};
+    float ms = 0.f;
+    for (int rep = 0; rep < 2; ++rep) {  // first launch warms, second is timed
+      cudaEventRecord(e0, st);
+      kF32X2Variants[v].direct(fast_trig, lofree, grid, st, a);
+      cudaEventRecord(e1, st);
+    }
+    cudaError_t e = cudaEventSynchronize(e1);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      return cuda_status(e, "two-vector pair-kernel tuning", __FILE__, __LINE__);
+    }
+    g_launches.fetch_add(2, std::memory_order_relaxed);
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best) {
+      best = ms;
+      f32x2_variant = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  nsplit_x2 = ns_v[f32x2_variant];
+  tuned_x2_ms = best;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune_x2_cache[key] = f32x2_variant;
+  return LUM_OK;
+}
+
+lum_status OtfOperator::apply2(int precision, const double2* x, const double2* x2, double2* y,
+                               double2* y2, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1,
+                               const int* skip, const int* skip2) {
+  if (has_lattice) {  // tabulated / per-pair Ewald operators: one vector at a time
+    LUM_TRY(apply(precision, x, y, st, ev0, ev1, skip));
+    return apply(precision, x2, y2, st, nullptr, nullptr, skip2);
+  }
+  if (!partial2.p) LUM_TRY(partial2.alloc(partial.bytes));
+  const int ntiles = (n + kOtfBlock - 1) / kOtfBlock;
+  const double s0 = k * k * k / (4.0 * kPi);
+  const int epi_blocks = (int)(((size_t)n * kEpiTPR + 255) / 256);
+  const double2 rr = make_double2(substrate.refl_re, substrate.refl_im);
+  const size_t slice = 3 * (size_t)n;
+  if (precision == LUM_FP32) {
+    if (f32x2_variant < 0) LUM_TRY(tune_f32_x2(st));
+    const F32X2VariantEntry& V = kF32X2Variants[f32x2_variant];
+    const int ns = nsplit_x2;
+    const int chunk = ((ntiles + ns - 1) / ns) * kOtfBlock;
+    dim3 grid((n + kOtfBlock * V.rows - 1) / (kOtfBlock * V.rows), ns);
+    const float2 one = make_float2(1.f, 0.f);
+    float2 *part = partial.as<float2>(), *part2 = partial2.as<float2>();
+    F32X2Args a{n, pos_hi.as<float4>(), pos_lo.as<float4>(), pos_hi.as<float4>(),
+                pos_lo.as<float4>(), x, x2, one, one, one, (float)k, (float)(1.0 / k),
+                (float)s0, chunk, part, part2, skip, skip2};
+    if (ev0) cudaEventRecord(ev0, st);
+    V.direct(fast_trig, lofree, grid, st, a);
+    LUM_CHECK_LAUNCH();
+    if (ev1) cudaEventRecord(ev1, st);
+    int nparts = ns;
+    if (has_substrate) {
+      F32X2Args b = a;
+      b.sh = img_hi.as<float4>();
+      b.sl = img_lo.as<float4>();
+      b.m0 = b.m1 = make_float2((float)-rr.x, (float)-rr.y);
+      b.m2 = make_float2((float)rr.x, (float)rr.y);
+      b.part = part + (size_t)ns * slice;
+      b.part2 = part2 + (size_t)ns * slice;
+      V.image(fast_trig, lofree && img_lofree, grid, st, b);
+      LUM_CHECK_LAUNCH();
+      nparts = 2 * ns;
+    }
+    otf_epilogue<float2, float2><<<epi_blocks, 256, 0, st>>>(
+        n, x, inv_alpha.as<double2>(), part, nparts, ell_w, near_j.as<int>(), fcd32.as<float2>(),
+        y, skip);
+    LUM_CHECK_LAUNCH();
+    otf_epilogue<float2, float2><<<epi_blocks, 256, 0, st>>>(
+        n, x2, inv_alpha.as<double2>(), part2, nparts, ell_w, near_j.as<int>(),
+        fcd32.as<float2>(), y2, skip2);
+    LUM_CHECK_LAUNCH();
+    return LUM_OK;
+  }
+  const int ns = nsplit64;
+  const int chunk = ((ntiles + ns - 1) / ns) * kOtfBlock;
+  dim3 grid(ntiles, ns);
+  const double2 one = make_double2(1.0, 0.0);
+  double2 *part = partial.as<double2>(), *part2 = partial2.as<double2>();
+  if (ev0) cudaEventRecord(ev0, st);
+  otf_pairs_f64_x2<false><<<grid, kOtfBlock, 0, st>>>(n, pos64.as<double4>(), x, x2, one, one, one,
+                                                      0.0, k, 1.0 / k, s0, chunk, part, part2,
+                                                      skip, skip2);
+  LUM_CHECK_LAUNCH();
+  if (ev1) cudaEventRecord(ev1, st);
+  int nparts = ns;
+  if (has_substrate) {
+    const double2 mneg = make_double2(-rr.x, -rr.y);
+    otf_pairs_f64_x2<true><<<grid, kOtfBlock, 0, st>>>(
+        n, pos64.as<double4>(), x, x2, mneg, mneg, rr, 2.0 * substrate.z_interface, k, 1.0 / k,
+        s0, chunk, part + (size_t)ns * slice, part2 + (size_t)ns * slice, skip, skip2);
+    LUM_CHECK_LAUNCH();
+    nparts = 2 * ns;
+  }
+  otf_epilogue<double2, double2><<<epi_blocks, 256, 0, st>>>(
+      n, x, inv_alpha.as<double2>(), part, nparts, ell_w, near_j.as<int>(), fcd64.as<double2>(),
+      y, skip);
+  LUM_CHECK_LAUNCH();
+  otf_epilogue<double2, double2><<<epi_blocks, 256, 0, st>>>(
+      n, x2, inv_alpha.as<double2>(), part2, nparts, ell_w, near_j.as<int>(),
+      fcd64.as<double2>(), y2, skip2);
+  LUM_CHECK_LAUNCH();
+  return LUM_OK;
+}
+
+// ---------------------------------------------------------------------------
 // Batched systems: K independent clusters concatenated into one dipole range
 // (BatchGeom).  Each pair kernel is one persistent launch over a work list of
 // (system, row tile, source split) items ordered by decreasing cost, drawn
@@ -939,10 +1216,10 @@ batch_pairs_f32(BatchGeom g, const double2* __restrict__ x, const int4* __restri
     const int chunk = g.sys_chunk32[s];
     const int j0 = item.z * chunk, j1 = min(n, j0 + chunk);
     const double k = g.sys_k[s];
-    pairs_f32_cta<FAST, false, LOFREE, 1>(
-        n, g.hi + off, g.lo + off, g.hi + off, g.lo + off, x + 3 * (size_t)off, one, one, one,
-        (float)k, (float)(1.0 / k), (float)(k * k * k / (4.0 * kPi)), item.y, j0, j1,
-        partial + (size_t)item.z * stride + 3 * (size_t)off);
+    pairs_f32_cta<FAST, false, LOFREE, 1, 1>(
+        n, g.hi + off, g.lo + off, g.hi + off, g.lo + off, x + 3 * (size_t)off, nullptr, one,
+        one, one, (float)k, (float)(1.0 / k), (float)(k * k * k / (4.0 * kPi)), item.y, j0, j1,
+        partial + (size_t)item.z * stride + 3 * (size_t)off, nullptr);
   }
 }
 
@@ -961,9 +1238,9 @@ batch_pairs_f64(BatchGeom g, const double2* __restrict__ x, const int4* __restri
     const int chunk = g.sys_chunk64[s];
     const int j0 = item.z * chunk, j1 = min(n, j0 + chunk);
     const double k = g.sys_k[s];
-    pairs_f64_cta<false>(n, g.pos64 + off, x + 3 * (size_t)off, one, one, one, 0.0, k, 1.0 / k,
-                         k * k * k / (4.0 * kPi), item.y, j0, j1,
-                         partial + (size_t)item.z * stride + 3 * (size_t)off);
+    pairs_f64_cta<false, 1>(n, g.pos64 + off, x + 3 * (size_t)off, nullptr, one, one, one, 0.0,
+                            k, 1.0 / k, k * k * k / (4.0 * kPi), item.y, j0, j1,
+                            partial + (size_t)item.z * stride + 3 * (size_t)off, nullptr);
   }
 }
 

@@ -14,6 +14,12 @@
 // LOFREE skips S5 and the lo terms when every centred position is exact in
 // FP32 (lo == 0), e.g. a lattice whose coordinates are multiples of 2^-k.
 //
+// NR = 2 applies the operator to two right-hand sides at once (e.g. the
+// forward and adjoint solves, or two polarisations): the tensor scalars A
+// and B' are evaluated once per pair and contracted with both source
+// vectors; the second vector adds three shared rows per source,
+//   S6 = (y0r,y0r,y0i,y0i)  S7 = (y1r,y1r,y1i,y1i)  S8 = (y2r,y2r,y2i,y2i).
+//
 // The self pair (j == i) only occurs in the two tiles that hold the CTA's
 // own rows; only those tiles run the masked loop.  The substrate image pass
 // (IMAGE) masks pairs whose image distance is below 1e-10 nm (r^2 < 1e-20).
@@ -32,11 +38,12 @@ __device__ __forceinline__ float2 sub2(float2 a, float2 b) {
   return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a);
 }
 
-template <bool FAST, bool IMAGE, bool LOFREE, bool CHECKED, int RP>
+template <bool FAST, bool IMAGE, bool LOFREE, bool CHECKED, int RP, int NR>
 __device__ __forceinline__ void pair_tile_f32x2(
     const float4 (*__restrict__ sS)[kOtfBlock], int cnt, int jt, const int* irow,
     const float2* OX, const float2* OY, const float2* OZ, const float2* LX, const float2* LY,
-    const float2* LZ, float2 (*acc)[6], float k, float2 inv_k2, float2 s02, float2 k2) {
+    const float2* LZ, float2 (*acc)[6], float2 (*acc2)[6], float k, float2 inv_k2, float2 s02,
+    float2 k2) {
 #pragma unroll 2
   for (int jj = 0; jj < cnt; ++jj) {
     const float4 S0 = sS[0][jj], S1 = sS[1][jj], S2 = sS[2][jj], S3 = sS[3][jj], S4 = sS[4][jj];
@@ -44,6 +51,14 @@ __device__ __forceinline__ void pair_tile_f32x2(
     if (!LOFREE) S5 = sS[5][jj];
     const float2 x0r = hi2(S1), x0i = lo2(S2), x1r = hi2(S2), x1i = lo2(S3), x2r = hi2(S3),
                  x2i = lo2(S4);
+    float4 S6 = make_float4(0.f, 0.f, 0.f, 0.f), S7 = S6, S8 = S6;
+    if constexpr (NR == 2) {
+      S6 = sS[6][jj];
+      S7 = sS[7][jj];
+      S8 = sS[8][jj];
+    }
+    const float2 y0r = lo2(S6), y0i = hi2(S6), y1r = lo2(S7), y1i = hi2(S7), y2r = lo2(S8),
+                 y2i = hi2(S8);
     const int j = jt + jj;
 #pragma unroll
     for (int p = 0; p < RP; ++p) {
@@ -99,26 +114,40 @@ __device__ __forceinline__ void pair_tile_f32x2(
       acc[p][3] = fma2(ti, dy, fma2(Ar, x1i, fma2(Ai, x1r, acc[p][3])));
       acc[p][4] = fma2(tr, dz, fma2(Ar, x2r, fma2(nAi, x2i, acc[p][4])));
       acc[p][5] = fma2(ti, dz, fma2(Ar, x2i, fma2(Ai, x2r, acc[p][5])));
+      if constexpr (NR == 2) {
+        const float2 dyr = fma2(dx, y0r, fma2(dy, y1r, mul2(dz, y2r)));
+        const float2 dyi = fma2(dx, y0i, fma2(dy, y1i, mul2(dz, y2i)));
+        const float2 ur = sub2(mul2(Br, dyr), mul2(Bi, dyi));
+        const float2 ui = fma2(Br, dyi, mul2(Bi, dyr));
+        acc2[p][0] = fma2(ur, dx, fma2(Ar, y0r, fma2(nAi, y0i, acc2[p][0])));
+        acc2[p][1] = fma2(ui, dx, fma2(Ar, y0i, fma2(Ai, y0r, acc2[p][1])));
+        acc2[p][2] = fma2(ur, dy, fma2(Ar, y1r, fma2(nAi, y1i, acc2[p][2])));
+        acc2[p][3] = fma2(ui, dy, fma2(Ar, y1i, fma2(Ai, y1r, acc2[p][3])));
+        acc2[p][4] = fma2(ur, dz, fma2(Ar, y2r, fma2(nAi, y2i, acc2[p][4])));
+        acc2[p][5] = fma2(ui, dz, fma2(Ar, y2i, fma2(Ai, y2r, acc2[p][5])));
+      }
     }
   }
 }
 
 // One CTA's work: rows [row0, row0 + 256*RP) of a system of n dipoles against
 // sources [j_begin, j_end); out[3i + c] = sum_j G(r_i - r_j) x'_j for the
-// CTA's rows (out is this split's slice of the partial buffer).  Shared by
-// the single-system kernel below and the batched kernel (batch.cu).
-template <bool FAST, bool IMAGE, bool LOFREE, int RP>
+// CTA's rows (out is this split's slice of the partial buffer), and the same
+// for x2 into out2 when NR == 2.  Shared by the single-system kernel below
+// and the batched kernel.
+template <bool FAST, bool IMAGE, bool LOFREE, int RP, int NR>
 __device__ __forceinline__ void pairs_f32_cta(
     int n, const float4* __restrict__ obs_hi, const float4* __restrict__ obs_lo,
     const float4* __restrict__ src_hi, const float4* __restrict__ src_lo,
-    const double2* __restrict__ x, float2 m0, float2 m1, float2 m2, float k, float inv_k,
-    float s0, int row0, int j_begin, int j_end, float2* __restrict__ out) {
+    const double2* __restrict__ x, const double2* __restrict__ x2, float2 m0, float2 m1,
+    float2 m2, float k, float inv_k, float s0, int row0, int j_begin, int j_end,
+    float2* __restrict__ out, float2* __restrict__ out2) {
   constexpr int ROWS = 2 * RP;
-  __shared__ float4 sS[6][kOtfBlock];
+  __shared__ float4 sS[NR == 2 ? 9 : 6][kOtfBlock];
   const int tid = threadIdx.x;
   int irow[ROWS];
   float2 OX[RP], OY[RP], OZ[RP], LX[RP], LY[RP], LZ[RP];
-  float2 acc[RP][6];
+  float2 acc[RP][6], acc2[NR == 2 ? RP : 1][6];
 #pragma unroll
   for (int p = 0; p < RP; ++p) {
     const int ia = row0 + (2 * p) * kOtfBlock + tid, ib = ia + kOtfBlock;
@@ -138,13 +167,17 @@ __device__ __forceinline__ void pairs_f32_cta(
     }
 #pragma unroll
     for (int c = 0; c < 6; ++c) acc[p][c] = f2(0.f, 0.f);
+    if constexpr (NR == 2) {
+#pragma unroll
+      for (int c = 0; c < 6; ++c) acc2[p][c] = f2(0.f, 0.f);
+    }
   }
   const float2 inv_k2 = f2(inv_k, inv_k), s02 = f2(s0, s0), k2 = f2(k, k);
   const int row_end = row0 + kOtfBlock * ROWS;
   // Software pipeline: the source of the next tile is loaded into registers
   // before the current tile is computed, hiding its global-load latency.
   float4 nh = make_float4(0.f, 0.f, 0.f, 0.f), nl = nh;
-  double2 na = make_double2(0.0, 0.0), nb = na, nc = na;
+  double2 na = make_double2(0.0, 0.0), nb = na, nc = na, nd = na, ne = na, nf = na;
   if (j_begin < j_end && tid < min(kOtfBlock, j_end - j_begin)) {
     const int j = j_begin + tid;
     nh = src_hi[j];
@@ -152,6 +185,11 @@ __device__ __forceinline__ void pairs_f32_cta(
     na = x[3 * j];
     nb = x[3 * j + 1];
     nc = x[3 * j + 2];
+    if constexpr (NR == 2) {
+      nd = x2[3 * j];
+      ne = x2[3 * j + 1];
+      nf = x2[3 * j + 2];
+    }
   }
   for (int jt = j_begin; jt < j_end; jt += kOtfBlock) {
     const int cnt = min(kOtfBlock, j_end - jt);
@@ -170,6 +208,18 @@ __device__ __forceinline__ void pairs_f32_cta(
       sS[3][tid] = make_float4(xb.y, xb.y, xc.x, xc.x);
       sS[4][tid] = make_float4(xc.y, xc.y, nl.x, nl.x);
       sS[5][tid] = make_float4(nl.y, nl.y, nl.z, nl.z);
+      if constexpr (NR == 2) {
+        float2 ya = f2((float)nd.x, (float)nd.y), yb = f2((float)ne.x, (float)ne.y),
+               yc = f2((float)nf.x, (float)nf.y);
+        if (IMAGE) {
+          ya = f2(m0.x * ya.x - m0.y * ya.y, m0.x * ya.y + m0.y * ya.x);
+          yb = f2(m1.x * yb.x - m1.y * yb.y, m1.x * yb.y + m1.y * yb.x);
+          yc = f2(m2.x * yc.x - m2.y * yc.y, m2.x * yc.y + m2.y * yc.x);
+        }
+        sS[6][tid] = make_float4(ya.x, ya.x, ya.y, ya.y);
+        sS[7][tid] = make_float4(yb.x, yb.x, yb.y, yb.y);
+        sS[8][tid] = make_float4(yc.x, yc.x, yc.y, yc.y);
+      }
     }
     __syncthreads();
     {
@@ -181,15 +231,20 @@ __device__ __forceinline__ void pairs_f32_cta(
         na = x[3 * j];
         nb = x[3 * j + 1];
         nc = x[3 * j + 2];
+        if constexpr (NR == 2) {
+          nd = x2[3 * j];
+          ne = x2[3 * j + 1];
+          nf = x2[3 * j + 2];
+        }
       }
     }
     const bool diag = IMAGE || (jt < row_end && jt + kOtfBlock > row0);  // CTA-uniform
     if (diag)
-      pair_tile_f32x2<FAST, IMAGE, LOFREE, true, RP>(sS, cnt, jt, irow, OX, OY, OZ, LX, LY, LZ,
-                                                     acc, k, inv_k2, s02, k2);
+      pair_tile_f32x2<FAST, IMAGE, LOFREE, true, RP, NR>(sS, cnt, jt, irow, OX, OY, OZ, LX, LY,
+                                                         LZ, acc, acc2, k, inv_k2, s02, k2);
     else
-      pair_tile_f32x2<FAST, IMAGE, LOFREE, false, RP>(sS, cnt, jt, irow, OX, OY, OZ, LX, LY,
-                                                      LZ, acc, k, inv_k2, s02, k2);
+      pair_tile_f32x2<FAST, IMAGE, LOFREE, false, RP, NR>(sS, cnt, jt, irow, OX, OY, OZ, LX, LY,
+                                                          LZ, acc, acc2, k, inv_k2, s02, k2);
   }
 #pragma unroll
   for (int p = 0; p < RP; ++p) {
@@ -198,12 +253,22 @@ __device__ __forceinline__ void pairs_f32_cta(
       out[3 * i + 0] = f2(acc[p][0].x, acc[p][1].x);
       out[3 * i + 1] = f2(acc[p][2].x, acc[p][3].x);
       out[3 * i + 2] = f2(acc[p][4].x, acc[p][5].x);
+      if constexpr (NR == 2) {
+        out2[3 * i + 0] = f2(acc2[p][0].x, acc2[p][1].x);
+        out2[3 * i + 1] = f2(acc2[p][2].x, acc2[p][3].x);
+        out2[3 * i + 2] = f2(acc2[p][4].x, acc2[p][5].x);
+      }
     }
     if (irow[2 * p + 1] < n) {
       const int i = irow[2 * p + 1];
       out[3 * i + 0] = f2(acc[p][0].y, acc[p][1].y);
       out[3 * i + 1] = f2(acc[p][2].y, acc[p][3].y);
       out[3 * i + 2] = f2(acc[p][4].y, acc[p][5].y);
+      if constexpr (NR == 2) {
+        out2[3 * i + 0] = f2(acc2[p][0].y, acc2[p][1].y);
+        out2[3 * i + 1] = f2(acc2[p][2].y, acc2[p][3].y);
+        out2[3 * i + 2] = f2(acc2[p][4].y, acc2[p][5].y);
+      }
     }
   }
 }
@@ -218,10 +283,37 @@ otf_pairs_f32(int n, const float4* __restrict__ obs_hi, const float4* __restrict
               const int* __restrict__ skip) {
   if (skip && *skip) return;  // CTA-uniform: the solve no longer needs this product
   const int j_begin = blockIdx.y * chunk;
-  pairs_f32_cta<FAST, IMAGE, LOFREE, RP>(n, obs_hi, obs_lo, src_hi, src_lo, x, m0, m1, m2, k,
-                                         inv_k, s0, blockIdx.x * (kOtfBlock * 2 * RP), j_begin,
-                                         min(n, j_begin + chunk),
-                                         partial + (size_t)blockIdx.y * (3 * (size_t)n));
+  pairs_f32_cta<FAST, IMAGE, LOFREE, RP, 1>(
+      n, obs_hi, obs_lo, src_hi, src_lo, x, nullptr, m0, m1, m2, k, inv_k, s0,
+      blockIdx.x * (kOtfBlock * 2 * RP), j_begin, min(n, j_begin + chunk),
+      partial + (size_t)blockIdx.y * (3 * (size_t)n), nullptr);
+}
+
+// Two right-hand sides with their own skip flags: both live -> one pass that
+// shares the tensor evaluation; one live -> the single-vector pass on it.
+// partial / partial2 receive the splits of x / x2.
+template <bool FAST, bool IMAGE, bool LOFREE, int RP, int MINB>
+__global__ void __launch_bounds__(kOtfBlock, MINB)
+otf_pairs_f32_x2(int n, const float4* __restrict__ obs_hi, const float4* __restrict__ obs_lo,
+                 const float4* __restrict__ src_hi, const float4* __restrict__ src_lo,
+                 const double2* __restrict__ x, const double2* __restrict__ x2, float2 m0,
+                 float2 m1, float2 m2, float k, float inv_k, float s0, int chunk,
+                 float2* __restrict__ partial, float2* __restrict__ partial2,
+                 const int* __restrict__ skip, const int* __restrict__ skip2) {
+  const bool live = !(skip && *skip), live2 = !(skip2 && *skip2);  // CTA-uniform
+  if (!live && !live2) return;
+  const int j_begin = blockIdx.y * chunk, j_end = min(n, j_begin + chunk);
+  const int row0 = blockIdx.x * (kOtfBlock * 2 * RP);
+  const size_t off = (size_t)blockIdx.y * (3 * (size_t)n);
+  if (live && live2)
+    pairs_f32_cta<FAST, IMAGE, LOFREE, RP, 2>(n, obs_hi, obs_lo, src_hi, src_lo, x, x2, m0, m1,
+                                              m2, k, inv_k, s0, row0, j_begin, j_end,
+                                              partial + off, partial2 + off);
+  else
+    pairs_f32_cta<FAST, IMAGE, LOFREE, RP, 1>(n, obs_hi, obs_lo, src_hi, src_lo,
+                                              live ? x : x2, nullptr, m0, m1, m2, k, inv_k, s0,
+                                              row0, j_begin, j_end,
+                                              (live ? partial : partial2) + off, nullptr);
 }
 
 }  // namespace lum
