@@ -153,9 +153,26 @@ LUM_API int lum_session_set_wavelength(lum_session* s, double k, const double* i
 LUM_API int lum_session_matvec(lum_session* s, int precision, const double* x, double* y);
 LUM_API int lum_session_matvec_device(lum_session* s, int precision, const void* x_dev, void* y_dev,
                               void* stream);
-/* Multi-RHS cached matvec Y = A X, X and Y row-major dim x nrhs (device). */
+/* Multi-RHS cached matvec Y = A X, X and Y row-major dim x nrhs (device).
+ * Method as LUM_MATMUL_AUTO below. */
 LUM_API int lum_session_matmul_device(lum_session* s, const void* X_dev, void* Y_dev, int nrhs,
                               void* stream);
+/* Methods of a multi-RHS cached product.  TENSOR runs on the tensor cores
+ * (tcgen05, TF32 operands split hi + lo, three products per pair: about FP32
+ * accuracy) and needs FP32 matrix storage; CUDA_CORES streams the matrix once
+ * per 8 vectors with FP64 accumulation; AUTO takes TENSOR for FP32 storage
+ * and nrhs >= 4. */
+enum { LUM_MATMUL_AUTO = 0, LUM_MATMUL_TENSOR = 1, LUM_MATMUL_CUDA_CORES = 2 };
+/* No single counterpart in the reference, which applies the cached matrix
+ * one vector per MatvecSession::matvec call (backend.rs:54, gpu.rs:428-488):
+ * Y = A X for nrhs vectors stored back to back (vector r at 3N*r complex,
+ * the layout of lum_solve_gmres_multi).  The device variant runs on `stream`
+ * (NULL = the session stream) without synchronising; the host variant
+ * synchronises and returns TIMEOUT if a tensor-core pipeline wait gave up. */
+LUM_API int lum_session_matmul_vectors_device(lum_session* s, const void* X_dev, void* Y_dev,
+                                              int nrhs, int method, void* stream);
+LUM_API int lum_session_matmul_vectors(lum_session* s, const double* X, double* Y, int nrhs,
+                                       int method);
 /* Use the caller's stream for all later work of this session (NULL resets). */
 LUM_API int lum_session_set_stream(lum_session* s, void* stream);
 LUM_API int lum_session_destroy(lum_session* s);

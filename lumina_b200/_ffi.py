@@ -83,6 +83,9 @@ SIGNATURES = {
     "lum_session_matvec": (c_int, [c_void_p, c_int, _dp, _dp]),
     "lum_session_matvec_device": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
     "lum_session_matmul_device": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
+    "lum_session_matmul_vectors_device": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int,
+                                                  c_void_p]),
+    "lum_session_matmul_vectors": (c_int, [c_void_p, _dp, _dp, c_int, c_int]),
     "lum_session_set_stream": (c_int, [c_void_p, c_void_p]),
     "lum_session_destroy": (c_int, [c_void_p]),
     "lum_solve_gmres": (c_int, [c_void_p, _dp, c_double, c_int, c_int, c_int, _dp,

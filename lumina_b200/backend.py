@@ -203,6 +203,30 @@ class CudaSession:
         _raise(self._lib.lum_session_matmul_device(self._h, c_void_p(X_ptr), c_void_p(Y_ptr),
                                                    nrhs, c_void_p(stream or None)), "matmul")
 
+    _METHODS = {"auto": 0, "tensor": 1, "cuda_cores": 2}
+
+    def matmul(self, X: np.ndarray, method="auto") -> np.ndarray:
+        """Y = A X for the columns of X (dim x nrhs) of a cached session: the
+        tensor cores (3xTF32) for FP32 storage, or the CUDA cores."""
+        Xc = _c128(X)
+        if Xc.ndim != 2 or Xc.shape[0] != self.dim:
+            raise DeviceError(f"Session dim={self.dim}, got X of shape {Xc.shape}")
+        nrhs = Xc.shape[1]
+        Xv = np.ascontiguousarray(Xc.T)  # vectors back to back
+        Yv = np.empty_like(Xv)
+        _raise(self._lib.lum_session_matmul_vectors(self._h, _dp(Xv.view(np.float64)),
+                                                    _dp(Yv.view(np.float64)), nrhs,
+                                                    self._METHODS[method]), "matmul")
+        return Yv.T
+
+    def matmul_vectors_device(self, X_ptr: int, Y_ptr: int, nrhs: int, method="auto",
+                              stream: int = 0) -> None:
+        """Y = A X for nrhs device vectors stored back to back (no synchronisation)."""
+        _raise(self._lib.lum_session_matmul_vectors_device(self._h, c_void_p(X_ptr),
+                                                           c_void_p(Y_ptr), nrhs,
+                                                           self._METHODS[method],
+                                                           c_void_p(stream or None)), "matmul")
+
     def set_stream(self, stream: int) -> None:
         _raise(self._lib.lum_session_set_stream(self._h, c_void_p(stream or None)), "set_stream")
 
@@ -314,10 +338,13 @@ class CudaSession:
         _raise(self._lib.lum_session_profile(self._h, int(enable)), "profile")
 
     def kernel_time(self, precision="fp32"):
-        """(launches, total ms) of the dominant kernel at ``precision`` since
+        """(launches, total ms) of the dominant kernel at ``precision`` ("fp32",
+        "fp64", or "fp32x2" / "fp64x2" for the two-vector kernels) since
         ``profile()`` was last called."""
         n, ms = c_int(0), c_double(0.0)
-        _raise(self._lib.lum_session_kernel_time(self._h, _prec(precision), byref(n), byref(ms)),
+        # "fp32x2" / "fp64x2": the two-vector pair kernels (recorded under precision + 2)
+        code = _prec(precision[:-2]) + 2 if str(precision).endswith("x2") else _prec(precision)
+        _raise(self._lib.lum_session_kernel_time(self._h, code, byref(n), byref(ms)),
                "kernel_time")
         return n.value, ms.value
 

@@ -33,12 +33,11 @@ __global__ void __launch_bounds__(128)
 assemble_pairs(int n, const double4* __restrict__ pos, const double2* __restrict__ inv_alpha,
                double k, int has_lat, LatticeDev L, const double4* __restrict__ lreal,
                const double4* __restrict__ lrecip, double kb0, double kb1, double kb2,
-               int has_sub, SubstrateDev sub, T2* __restrict__ A) {
+               int has_sub, SubstrateDev sub, size_t ld, T2* __restrict__ A) {
   const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long npairs = (long long)n * n;
   if (idx >= npairs) return;
   const int i = (int)(idx / n), j = (int)(idx % n);
-  const size_t dim = 3 * (size_t)n;
   const double4 ri = pos[i], rj = pos[j];
   const double kb[3] = {kb0, kb1, kb2};
   double2 blk[9];
@@ -79,23 +78,22 @@ assemble_pairs(int n, const double4* __restrict__ pos, const double2* __restrict
   }
   for (int a = 0; a < 3; ++a)
     for (int b = 0; b < 3; ++b)
-      A[(3 * (size_t)i + a) * dim + 3 * (size_t)j + b] = mk<T2>(blk[3 * a + b].x, blk[3 * a + b].y);
+      A[(3 * (size_t)i + a) * ld + 3 * (size_t)j + b] = mk<T2>(blk[3 * a + b].x, blk[3 * a + b].y);
 }
 
 // FCD: A[i][j] -= (G_fcd - G_point) for every near pair.
 template <typename T2>
 __global__ void assemble_fcd(int n, int ell_w, const int* __restrict__ near_j,
-                             const double2* __restrict__ fcd, T2* __restrict__ A) {
+                             const double2* __restrict__ fcd, size_t ld, T2* __restrict__ A) {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= n * ell_w) return;
   const int w = idx / n, i = idx % n;
   const int j = near_j[(size_t)w * n + i];
   if (j < 0) return;
-  const size_t dim = 3 * (size_t)n;
   for (int a = 0; a < 3; ++a)
     for (int b = 0; b < 3; ++b) {
       const double2 c = fcd[((size_t)w * 9 + 3 * a + b) * n + i];
-      T2& e = A[(3 * (size_t)i + a) * dim + 3 * (size_t)j + b];
+      T2& e = A[(3 * (size_t)i + a) * ld + 3 * (size_t)j + b];
       e = mk<T2>((double)e.x - c.x, (double)e.y - c.y);
     }
 }
@@ -103,13 +101,13 @@ __global__ void assemble_fcd(int n, int ell_w, const int* __restrict__ near_j,
 // y = A x; one warp per row, 4 independent loads in flight per lane.
 template <typename T2>
 __global__ void __launch_bounds__(256)
-gemv_rows(int dim, const T2* __restrict__ A, const double2* __restrict__ x,
+gemv_rows(int dim, size_t ld, const T2* __restrict__ A, const double2* __restrict__ x,
           double2* __restrict__ y, const int* __restrict__ skip) {
   if (skip && *skip) return;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= dim) return;
-  const T2* row = A + (size_t)warp * dim;
+  const T2* row = A + (size_t)warp * ld;
   double sr = 0.0, si = 0.0;
   int c = lane;
   for (; c + 96 < dim; c += 128) {
@@ -137,25 +135,27 @@ gemv_rows(int dim, const T2* __restrict__ A, const double2* __restrict__ x,
   if (lane == 0) y[warp] = make_double2(sr, si);
 }
 
-// Y = A X for nrhs right-hand sides (X, Y row-major dim x nrhs): one warp
-// per row, A read once and applied to NR vectors held in registers.
+// Y = A X for nrhs right-hand sides on the CUDA cores: one warp per row, A
+// read once per NR vectors held in registers.  Element (c, r) of X is at
+// X[c * sc + r * sr] (row-major dim x nrhs: sc = nrhs, sr = 1; vectors back to
+// back: sc = 1, sr = dim), and the same strides address Y.
 template <typename T2, int NR>
 __global__ void __launch_bounds__(256)
-gemm_rows(int dim, const T2* __restrict__ A, const double2* __restrict__ X, int nrhs, int c0,
-          double2* __restrict__ Y) {
+gemm_rows(int dim, size_t ld, const T2* __restrict__ A, const double2* __restrict__ X,
+          long long sc, long long sr_, int c0, double2* __restrict__ Y) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= dim) return;
-  const T2* row = A + (size_t)warp * dim;
+  const T2* row = A + (size_t)warp * ld;
   double sr[NR], si[NR];
 #pragma unroll
   for (int r = 0; r < NR; ++r) sr[r] = si[r] = 0.0;
   for (int c = lane; c < dim; c += 32) {
     T2 a = row[c];
-    const double2* xr = X + (size_t)c * nrhs + c0;
+    const double2* xr = X + (long long)c * sc + (long long)c0 * sr_;
 #pragma unroll
     for (int r = 0; r < NR; ++r) {
-      double2 xv = __ldg(&xr[r]);
+      double2 xv = __ldg(&xr[r * sr_]);
       sr[r] += (double)a.x * xv.x - (double)a.y * xv.y;
       si[r] += (double)a.x * xv.y + (double)a.y * xv.x;
     }
@@ -166,30 +166,41 @@ gemm_rows(int dim, const T2* __restrict__ A, const double2* __restrict__ X, int 
       sr[r] += __shfl_down_sync(0xffffffffu, sr[r], o);
       si[r] += __shfl_down_sync(0xffffffffu, si[r], o);
     }
-    if (lane == 0) Y[(size_t)warp * nrhs + c0 + r] = make_double2(sr[r], si[r]);
+    if (lane == 0) Y[(long long)warp * sc + (long long)(c0 + r) * sr_] = make_double2(sr[r], si[r]);
   }
 }
 
-__global__ void narrow_rows(size_t count, const double2* __restrict__ src, float2* __restrict__ dst) {
+// FP64 rows (dense, dim entries each) -> FP32 rows of pitch ld.
+__global__ void narrow_rows(size_t rows, int dim, const double2* __restrict__ src, size_t ld,
+                            float2* __restrict__ dst) {
+  const size_t count = rows * dim;
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < count;
        q += (size_t)gridDim.x * blockDim.x) {
-    double2 v = src[q];
-    dst[q] = make_float2((float)v.x, (float)v.y);
+    const size_t r = q / dim, c = q % dim;
+    const double2 v = src[q];
+    dst[r * ld + c] = make_float2((float)v.x, (float)v.y);
   }
 }
 
 lum_status CachedOperator::allocate(int dim_, int precision_) {
   dim = dim_;
   precision = precision_;
-  size_t es = (precision == LUM_FP32) ? sizeof(float2) : sizeof(double2);
-  LUM_TRY(A.alloc(es * (size_t)dim * dim));
+  // Rows are padded to a multiple of 16 complex entries (128 B in FP32):
+  // every row starts 128-byte aligned, and the tensor-core GEMM reads the
+  // matrix through a TMA map whose row pitch must be a multiple of 16 bytes.
+  // The padding is zero so that it contributes nothing to a product.
+  ld = ((size_t)dim + 15) / 16 * 16;
+  const size_t es = (precision == LUM_FP32) ? sizeof(float2) : sizeof(double2);
+  LUM_TRY(A.alloc(es * ld * dim));
+  LUM_TRY_CUDA(cudaMemset(A.p, 0, es * ld * dim));
+  tc.release();
   return LUM_OK;
 }
 
 lum_status CachedOperator::upload(const double* host, cudaStream_t st) {
-  const size_t count = (size_t)dim * dim;
   if (precision == LUM_FP64) {
-    LUM_TRY_CUDA(cudaMemcpyAsync(A.p, host, sizeof(double2) * count, cudaMemcpyHostToDevice, st));
+    LUM_TRY_CUDA(cudaMemcpy2DAsync(A.p, sizeof(double2) * ld, host, sizeof(double2) * dim,
+                                   sizeof(double2) * dim, dim, cudaMemcpyHostToDevice, st));
     LUM_TRY_CUDA(cudaStreamSynchronize(st));
     return LUM_OK;
   }
@@ -199,11 +210,11 @@ lum_status CachedOperator::upload(const double* host, cudaStream_t st) {
   DevBuf stage;
   LUM_TRY(stage.alloc(sizeof(double2) * rows_per * dim));
   for (size_t r0 = 0; r0 < (size_t)dim; r0 += rows_per) {
-    size_t nr = std::min(rows_per, (size_t)dim - r0);
-    size_t cnt = nr * dim;
-    LUM_TRY_CUDA(cudaMemcpyAsync(stage.p, host + 2 * r0 * dim, sizeof(double2) * cnt,
+    const size_t nr = std::min(rows_per, (size_t)dim - r0);
+    LUM_TRY_CUDA(cudaMemcpyAsync(stage.p, host + 2 * r0 * dim, sizeof(double2) * nr * dim,
                                  cudaMemcpyHostToDevice, st));
-    narrow_rows<<<1024, 256, 0, st>>>(cnt, stage.as<double2>(), A.as<float2>() + r0 * dim);
+    narrow_rows<<<1024, 256, 0, st>>>(nr, dim, stage.as<double2>(), ld,
+                                      A.as<float2>() + r0 * ld);
     LUM_CHECK_LAUNCH();
   }
   LUM_TRY_CUDA(cudaStreamSynchronize(st));
@@ -219,26 +230,26 @@ lum_status CachedOperator::assemble(const OtfOperator& g, cudaStream_t st) {
     set_error("matrix too large for device assembly");
     return LUM_ERR_INVALID;
   }
-  if (g.has_lattice && g.table_ok) return assemble_from_table(g, precision, A.p, st);
+  if (g.has_lattice && g.table_ok) return assemble_from_table(g, precision, A.p, ld, st);
   if (precision == LUM_FP32)
     assemble_pairs<float2><<<(unsigned)blocks, threads, 0, st>>>(
         n, g.pos64.as<double4>(), g.inv_alpha.as<double2>(), g.k, g.has_lattice, g.latdev,
         g.lat_real.as<double4>(), g.lat_recip.as<double4>(), g.kbloch[0], g.kbloch[1],
-        g.kbloch[2], g.has_substrate, g.substrate, A.as<float2>());
+        g.kbloch[2], g.has_substrate, g.substrate, ld, A.as<float2>());
   else
     assemble_pairs<double2><<<(unsigned)blocks, threads, 0, st>>>(
         n, g.pos64.as<double4>(), g.inv_alpha.as<double2>(), g.k, g.has_lattice, g.latdev,
         g.lat_real.as<double4>(), g.lat_recip.as<double4>(), g.kbloch[0], g.kbloch[1],
-        g.kbloch[2], g.has_substrate, g.substrate, A.as<double2>());
+        g.kbloch[2], g.has_substrate, g.substrate, ld, A.as<double2>());
   LUM_CHECK_LAUNCH();
   if (g.ell_w > 0 && !g.has_lattice) {
     const int total = n * g.ell_w;
     if (precision == LUM_FP32)
       assemble_fcd<float2><<<(total + 255) / 256, 256, 0, st>>>(
-          n, g.ell_w, g.near_j.as<int>(), g.fcd64.as<double2>(), A.as<float2>());
+          n, g.ell_w, g.near_j.as<int>(), g.fcd64.as<double2>(), ld, A.as<float2>());
     else
       assemble_fcd<double2><<<(total + 255) / 256, 256, 0, st>>>(
-          n, g.ell_w, g.near_j.as<int>(), g.fcd64.as<double2>(), A.as<double2>());
+          n, g.ell_w, g.near_j.as<int>(), g.fcd64.as<double2>(), ld, A.as<double2>());
     LUM_CHECK_LAUNCH();
   }
   return LUM_OK;
@@ -248,25 +259,28 @@ lum_status CachedOperator::apply(const double2* x, double2* y, cudaStream_t st,
                                  const int* skip) {
   const int blocks = (int)(((size_t)dim * 32 + 255) / 256);
   if (precision == LUM_FP32)
-    gemv_rows<float2><<<blocks, 256, 0, st>>>(dim, A.as<float2>(), x, y, skip);
+    gemv_rows<float2><<<blocks, 256, 0, st>>>(dim, ld, A.as<float2>(), x, y, skip);
   else
-    gemv_rows<double2><<<blocks, 256, 0, st>>>(dim, A.as<double2>(), x, y, skip);
+    gemv_rows<double2><<<blocks, 256, 0, st>>>(dim, ld, A.as<double2>(), x, y, skip);
   LUM_CHECK_LAUNCH();
   return LUM_OK;
 }
 
-lum_status CachedOperator::apply_multi(const double2* X, double2* Y, int nrhs, cudaStream_t st) {
+lum_status CachedOperator::apply_multi_cuda_cores(const double2* X, double2* Y, int nrhs,
+                                                  long long sc, long long sr, cudaStream_t st) {
   const int blocks = (int)(((size_t)dim * 32 + 255) / 256);
   int c0 = 0;
   while (c0 < nrhs) {
     int left = nrhs - c0;
     int nr = left >= 8 ? 8 : (left >= 4 ? 4 : (left >= 2 ? 2 : 1));
-#define LUM_GEMM_CASE(NRV)                                                                  \
-  case NRV:                                                                                 \
-    if (precision == LUM_FP32)                                                              \
-      gemm_rows<float2, NRV><<<blocks, 256, 0, st>>>(dim, A.as<float2>(), X, nrhs, c0, Y);  \
-    else                                                                                    \
-      gemm_rows<double2, NRV><<<blocks, 256, 0, st>>>(dim, A.as<double2>(), X, nrhs, c0, Y); \
+#define LUM_GEMM_CASE(NRV)                                                                     \
+  case NRV:                                                                                    \
+    if (precision == LUM_FP32)                                                                 \
+      gemm_rows<float2, NRV><<<blocks, 256, 0, st>>>(dim, ld, A.as<float2>(), X, sc, sr, c0,   \
+                                                     Y);                                       \
+    else                                                                                       \
+      gemm_rows<double2, NRV><<<blocks, 256, 0, st>>>(dim, ld, A.as<double2>(), X, sc, sr, c0, \
+                                                      Y);                                      \
     break;
     switch (nr) {
       LUM_GEMM_CASE(8)
@@ -279,6 +293,18 @@ lum_status CachedOperator::apply_multi(const double2* X, double2* Y, int nrhs, c
     c0 += nr;
   }
   return LUM_OK;
+}
+
+lum_status CachedOperator::apply_multi(const double2* X, double2* Y, int nrhs, long long sc,
+                                       long long sr, int method, cudaStream_t st) {
+  const bool tensor = precision == LUM_FP32 &&
+                      (method == LUM_MATMUL_TENSOR || (method == LUM_MATMUL_AUTO && nrhs >= kTcMinRhs));
+  if (method == LUM_MATMUL_TENSOR && precision != LUM_FP32) {
+    set_error("the tensor-core product needs FP32 matrix storage");
+    return LUM_ERR_INVALID;
+  }
+  if (tensor) return cgemm_tf32x3(*this, X, sc, sr, Y, sc, sr, nrhs, st);
+  return apply_multi_cuda_cores(X, Y, nrhs, sc, sr, st);
 }
 
 }  // namespace lum

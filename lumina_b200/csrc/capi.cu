@@ -485,15 +485,50 @@ int lum_session_matvec(lum_session* s, int precision, const double* x, double* y
   return LUM_OK;
 }
 
-int lum_session_matmul_device(lum_session* s, const void* X, void* Y, int nrhs, void* stream) {
+static lum_status check_matmul(lum_session* s, const void* X, const void* Y, int nrhs,
+                               int method) {
   if (bad_ptr(s, "session") || bad_ptr(X, "X") || bad_ptr(Y, "Y")) return LUM_ERR_INVALID;
   if (s->kind != 1 || nrhs <= 0) {
     set_error("matmul needs a cached session and nrhs > 0");
     return LUM_ERR_INVALID;
   }
+  if (method != LUM_MATMUL_AUTO && method != LUM_MATMUL_TENSOR &&
+      method != LUM_MATMUL_CUDA_CORES) {
+    set_error("invalid matmul method %d", method);
+    return LUM_ERR_INVALID;
+  }
+  return LUM_OK;
+}
+
+int lum_session_matmul_device(lum_session* s, const void* X, void* Y, int nrhs, void* stream) {
+  LUM_TRY(check_matmul(s, X, Y, nrhs, LUM_MATMUL_AUTO));
   cudaSetDevice(s->ctx->device);
-  return s->cached.apply_multi((const double2*)X, (double2*)Y, nrhs,
+  return s->cached.apply_multi((const double2*)X, (double2*)Y, nrhs, nrhs, 1, LUM_MATMUL_AUTO,
                                stream ? (cudaStream_t)stream : s->stream);
+}
+
+int lum_session_matmul_vectors_device(lum_session* s, const void* X, void* Y, int nrhs,
+                                      int method, void* stream) {
+  LUM_TRY(check_matmul(s, X, Y, nrhs, method));
+  cudaSetDevice(s->ctx->device);
+  return s->cached.apply_multi((const double2*)X, (double2*)Y, nrhs, 1, s->dim, method,
+                               stream ? (cudaStream_t)stream : s->stream);
+}
+
+int lum_session_matmul_vectors(lum_session* s, const double* X, double* Y, int nrhs,
+                               int method) {
+  LUM_TRY(check_matmul(s, X, Y, nrhs, method));
+  cudaSetDevice(s->ctx->device);
+  const size_t bytes = sizeof(double2) * (size_t)s->dim * nrhs;
+  lum::DevBuf dx, dy;
+  LUM_TRY(dx.alloc(bytes));
+  LUM_TRY(dy.alloc(bytes));
+  LUM_TRY_CUDA(cudaMemcpyAsync(dx.p, X, bytes, cudaMemcpyHostToDevice, s->stream));
+  LUM_TRY(s->cached.apply_multi(dx.as<double2>(), dy.as<double2>(), nrhs, 1, s->dim, method,
+                                s->stream));
+  LUM_TRY_CUDA(cudaMemcpyAsync(Y, dy.p, bytes, cudaMemcpyDeviceToHost, s->stream));
+  LUM_TRY_CUDA(cudaStreamSynchronize(s->stream));
+  return lum::cgemm_status(s->cached, s->stream);
 }
 
 // nrhs right-hand sides of one session, two at a time in lockstep.

@@ -161,17 +161,56 @@ struct OtfOperator {
 };
 
 // --- cached (dense matrix) operator ----------------------------------------
+// Workspace of the tensor-core product (cgemm_tc.cu): the right-hand sides
+// split into TF32 hi/lo operands, split-K partial sums, the TMA maps and a
+// device status word.
+struct TcWork {
+  DevBuf bhi, blo;          // float [npad][2 ld] each (K-major B operand)
+  DevBuf part;              // float2 [ksplit][nrhs][dim] split-K partials
+  DevBuf status;            // int: nonzero after a pipeline wait gave up
+  int npad = 0;             // rows of bhi/blo the TMA maps describe
+  size_t part_bytes = 0;
+  const void* mapped_a = nullptr;
+  alignas(64) unsigned char map_a[128];
+  alignas(64) unsigned char map_bhi[128];
+  alignas(64) unsigned char map_blo[128];
+  void release() {
+    bhi.release();
+    blo.release();
+    part.release();
+    npad = 0;
+    part_bytes = 0;
+    mapped_a = nullptr;
+  }
+};
+
+// Right-hand sides from which the automatic method takes the tensor cores.
+constexpr int kTcMinRhs = 4;
+
 struct CachedOperator {
   int dim = 0;              // 3N
+  size_t ld = 0;            // row pitch in complex entries (dim rounded up to 16)
   int precision = LUM_FP32; // storage precision of A
-  DevBuf A;                 // float2 or double2 [dim][dim] row-major
+  DevBuf A;                 // float2 or double2 [dim][ld] row-major, zero padding
   DevBuf x32;               // float2[dim] staging for FP32 storage
+  TcWork tc;
   lum_status allocate(int dim, int precision);
   lum_status upload(const double* host, cudaStream_t st);
   lum_status assemble(const OtfOperator& geo, cudaStream_t st);
   lum_status apply(const double2* x, double2* y, cudaStream_t st, const int* skip = nullptr);
-  lum_status apply_multi(const double2* X, double2* Y, int nrhs, cudaStream_t st);
+  // Y = A X; element (c, r) of X and Y at [c * sc + r * sr].
+  lum_status apply_multi(const double2* X, double2* Y, int nrhs, long long sc, long long sr,
+                         int method, cudaStream_t st);
+  lum_status apply_multi_cuda_cores(const double2* X, double2* Y, int nrhs, long long sc,
+                                    long long sr, cudaStream_t st);
 };
+
+// Tensor-core product Y = A X of an FP32-storage cached matrix (cgemm_tc.cu).
+lum_status cgemm_tf32x3(CachedOperator& op, const double2* X, long long sxc, long long sxr,
+                        double2* Y, long long syc, long long syr, int nrhs, cudaStream_t st);
+// LUM_ERR_TIMEOUT when a pipeline wait of an earlier product gave up (and
+// clears the record); synchronises `st`.
+lum_status cgemm_status(CachedOperator& op, cudaStream_t st);
 
 // --- GMRES workspace --------------------------------------------------------
 struct GmresState {
@@ -255,7 +294,7 @@ lum_status batch_apply(const BatchGeom& g, int precision, const double2* x, doub
 int batch_occupancy(const BatchGeom& g, int precision);                              // otf.cu
 
 const char* f32_variant_name(int v);  // otf.cu
-lum_status assemble_from_table(const OtfOperator& g, int precision, void* A,
+lum_status assemble_from_table(const OtfOperator& g, int precision, void* A, size_t ld,
                                cudaStream_t st);  // table.cu
 
 // vector kernels (gmres.cu)

@@ -257,11 +257,10 @@ template <typename T2>
 __global__ void __launch_bounds__(128)
 assemble_table(int n, const int4* __restrict__ lidx, const double2* __restrict__ inv_alpha,
                const double2* __restrict__ tab, const double2* __restrict__ img, int Db, int Dc,
-               int oa, int ob, int oc, int Dcs, double2 rr, T2* __restrict__ A) {
+               int oa, int ob, int oc, int Dcs, double2 rr, size_t ld, T2* __restrict__ A) {
   const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (long long)n * n) return;
   const int i = (int)(idx / n), j = (int)(idx % n);
-  const size_t dim = 3 * (size_t)n;
   const int4 li = lidx[i], lj = lidx[j];
   const int ab = (li.x - lj.x + oa) * Db + (li.y - lj.y + ob);
   const double2* t = tab + ((size_t)ab * Dc + (li.z - lj.z + oc)) * kEntry;
@@ -279,12 +278,13 @@ assemble_table(int n, const int4* __restrict__ lidx, const double2* __restrict__
         v.x -= m[q].x * h.x - m[q].y * h.y;
         v.y -= m[q].x * h.y + m[q].y * h.x;
       }
-      A[(3 * (size_t)i + p) * dim + 3 * (size_t)j + q] = C2<typename std::conditional<
+      A[(3 * (size_t)i + p) * ld + 3 * (size_t)j + q] = C2<typename std::conditional<
           sizeof(T2) == sizeof(float2), float, double>::type>::mk(v.x, v.y);
     }
 }
 
-lum_status assemble_from_table(const OtfOperator& g, int precision, void* A, cudaStream_t st) {
+lum_status assemble_from_table(const OtfOperator& g, int precision, void* A, size_t ld,
+                               cudaStream_t st) {
   const long long npairs = (long long)g.n * g.n;
   const unsigned blocks = (unsigned)((npairs + 127) / 128);
   const int oa = g.tdim[0] / 2, ob = g.tdim[1] / 2, oc = g.tdim[2] / 2;
@@ -293,11 +293,11 @@ lum_status assemble_from_table(const OtfOperator& g, int precision, void* A, cud
   if (precision == LUM_FP32)
     assemble_table<float2><<<blocks, 128, 0, st>>>(
         g.n, g.lidx.as<int4>(), g.inv_alpha.as<double2>(), g.tab64.as<double2>(), img, g.tdim[1],
-        g.tdim[2], oa, ob, oc, g.tsdim, rr, static_cast<float2*>(A));
+        g.tdim[2], oa, ob, oc, g.tsdim, rr, ld, static_cast<float2*>(A));
   else
     assemble_table<double2><<<blocks, 128, 0, st>>>(
         g.n, g.lidx.as<int4>(), g.inv_alpha.as<double2>(), g.tab64.as<double2>(), img, g.tdim[1],
-        g.tdim[2], oa, ob, oc, g.tsdim, rr, static_cast<double2*>(A));
+        g.tdim[2], oa, ob, oc, g.tsdim, rr, ld, static_cast<double2*>(A));
   LUM_CHECK_LAUNCH();
   return LUM_OK;
 }
