@@ -98,41 +98,98 @@ __global__ void assemble_fcd(int n, int ell_w, const int* __restrict__ near_j,
     }
 }
 
-// y = A x; one warp per row, 4 independent loads in flight per lane.
+// y = A x in two launches.  gemv_part: one warp per (row, column chunk), the
+// chunk streamed with 16-byte loads (two FP32 complex or one FP64 complex per
+// load, four in flight per lane), FP64 accumulation, shuffle reduction, one
+// partial per chunk.  Many small blocks let the block scheduler balance the
+// SMs to the last wave.  gemv_reduce sums the chunks of a row in chunk order
+// (deterministic).
+constexpr int kGemvRows = 8;  // rows (warps) per block
+
+__device__ __forceinline__ void cmac(double& sr, double& si, float ar, float ai, double2 x) {
+  sr += (double)ar * x.x - (double)ai * x.y;
+  si += (double)ar * x.y + (double)ai * x.x;
+}
+
 template <typename T2>
 __global__ void __launch_bounds__(256)
-gemv_rows(int dim, size_t ld, const T2* __restrict__ A, const double2* __restrict__ x,
-          double2* __restrict__ y, const int* __restrict__ skip) {
+gemv_part(int dim, size_t ld, int chunk, const T2* __restrict__ A,
+          const double2* __restrict__ x, double2* __restrict__ part,
+          const int* __restrict__ skip) {
   if (skip && *skip) return;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int row = blockIdx.x * kGemvRows + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
-  if (warp >= dim) return;
-  const T2* row = A + (size_t)warp * ld;
+  if (row >= dim) return;
+  const int c0 = blockIdx.y * chunk, c1 = min(dim, c0 + chunk);
+  const T2* a = A + (size_t)row * ld;
   double sr = 0.0, si = 0.0;
-  int c = lane;
-  for (; c + 96 < dim; c += 128) {
-    T2 a0 = row[c], a1 = row[c + 32], a2 = row[c + 64], a3 = row[c + 96];
-    double2 x0 = __ldg(&x[c]), x1 = __ldg(&x[c + 32]), x2 = __ldg(&x[c + 64]), x3 = __ldg(&x[c + 96]);
-    sr += (double)a0.x * x0.x - (double)a0.y * x0.y;
-    si += (double)a0.x * x0.y + (double)a0.y * x0.x;
-    sr += (double)a1.x * x1.x - (double)a1.y * x1.y;
-    si += (double)a1.x * x1.y + (double)a1.y * x1.x;
-    sr += (double)a2.x * x2.x - (double)a2.y * x2.y;
-    si += (double)a2.x * x2.y + (double)a2.y * x2.x;
-    sr += (double)a3.x * x3.x - (double)a3.y * x3.y;
-    si += (double)a3.x * x3.y + (double)a3.y * x3.x;
-  }
-  for (; c < dim; c += 32) {
-    T2 a0 = row[c];
-    double2 x0 = __ldg(&x[c]);
-    sr += (double)a0.x * x0.x - (double)a0.y * x0.y;
-    si += (double)a0.x * x0.y + (double)a0.y * x0.x;
+  if constexpr (sizeof(T2) == sizeof(float2)) {
+    // float4 p holds complex 2p and 2p+1 (rows start 128-byte aligned, c0 even)
+    const float4* a4 = reinterpret_cast<const float4*>(a);
+    const int p1 = c1 >> 1;
+    int p = (c0 >> 1) + lane;
+    for (; p + 96 < p1; p += 128) {
+      const float4 v0 = __ldcs(&a4[p]), v1 = __ldcs(&a4[p + 32]), v2 = __ldcs(&a4[p + 64]),
+                   v3 = __ldcs(&a4[p + 96]);
+      cmac(sr, si, v0.x, v0.y, __ldg(&x[2 * p]));
+      cmac(sr, si, v0.z, v0.w, __ldg(&x[2 * p + 1]));
+      cmac(sr, si, v1.x, v1.y, __ldg(&x[2 * p + 64]));
+      cmac(sr, si, v1.z, v1.w, __ldg(&x[2 * p + 65]));
+      cmac(sr, si, v2.x, v2.y, __ldg(&x[2 * p + 128]));
+      cmac(sr, si, v2.z, v2.w, __ldg(&x[2 * p + 129]));
+      cmac(sr, si, v3.x, v3.y, __ldg(&x[2 * p + 192]));
+      cmac(sr, si, v3.z, v3.w, __ldg(&x[2 * p + 193]));
+    }
+    for (; p < p1; p += 32) {
+      const float4 v = __ldcs(&a4[p]);
+      cmac(sr, si, v.x, v.y, __ldg(&x[2 * p]));
+      cmac(sr, si, v.z, v.w, __ldg(&x[2 * p + 1]));
+    }
+    if ((c1 & 1) && lane == 0) {  // odd last column of the row
+      const float2 v = a[c1 - 1];
+      cmac(sr, si, v.x, v.y, __ldg(&x[c1 - 1]));
+    }
+  } else {
+    int c = c0 + lane;
+    for (; c + 96 < c1; c += 128) {
+      const double2 a0 = __ldcs(&a[c]), a1 = __ldcs(&a[c + 32]), a2 = __ldcs(&a[c + 64]),
+                    a3 = __ldcs(&a[c + 96]);
+      const double2 x0 = __ldg(&x[c]), x1 = __ldg(&x[c + 32]), x2 = __ldg(&x[c + 64]),
+                    x3 = __ldg(&x[c + 96]);
+      sr += a0.x * x0.x - a0.y * x0.y;
+      si += a0.x * x0.y + a0.y * x0.x;
+      sr += a1.x * x1.x - a1.y * x1.y;
+      si += a1.x * x1.y + a1.y * x1.x;
+      sr += a2.x * x2.x - a2.y * x2.y;
+      si += a2.x * x2.y + a2.y * x2.x;
+      sr += a3.x * x3.x - a3.y * x3.y;
+      si += a3.x * x3.y + a3.y * x3.x;
+    }
+    for (; c < c1; c += 32) {
+      const double2 a0 = __ldcs(&a[c]), x0 = __ldg(&x[c]);
+      sr += a0.x * x0.x - a0.y * x0.y;
+      si += a0.x * x0.y + a0.y * x0.x;
+    }
   }
   for (int o = 16; o > 0; o >>= 1) {
     sr += __shfl_down_sync(0xffffffffu, sr, o);
     si += __shfl_down_sync(0xffffffffu, si, o);
   }
-  if (lane == 0) y[warp] = make_double2(sr, si);
+  if (lane == 0) part[(size_t)blockIdx.y * dim + row] = make_double2(sr, si);
+}
+
+__global__ void gemv_reduce(int dim, int nchunks, const double2* __restrict__ part,
+                            double2* __restrict__ y, const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= dim) return;
+  double sr = 0.0, si = 0.0;
+  for (int c = 0; c < nchunks; ++c) {
+    const double2 v = part[(size_t)c * dim + row];
+    sr += v.x;
+    si += v.y;
+  }
+  y[row] = make_double2(sr, si);
 }
 
 // Y = A X for nrhs right-hand sides on the CUDA cores: one warp per row, A
@@ -194,6 +251,7 @@ lum_status CachedOperator::allocate(int dim_, int precision_) {
   LUM_TRY(A.alloc(es * ld * dim));
   LUM_TRY_CUDA(cudaMemset(A.p, 0, es * ld * dim));
   tc.release();
+  gemv_chunks = 0;
   return LUM_OK;
 }
 
@@ -257,11 +315,29 @@ lum_status CachedOperator::assemble(const OtfOperator& g, cudaStream_t st) {
 
 lum_status CachedOperator::apply(const double2* x, double2* y, cudaStream_t st,
                                  const int* skip) {
-  const int blocks = (int)(((size_t)dim * 32 + 255) / 256);
+  if (gemv_chunks == 0) {
+    // about 8 waves of 8-warp blocks (8 resident per SM), chunks of >= 512
+    // complex entries, an even chunk length (16-byte loads of FP32 pairs)
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int row_blocks = (dim + kGemvRows - 1) / kGemvRows;
+    const int want = std::max(1, (8 * 8 * sms + row_blocks - 1) / row_blocks);
+    gemv_chunks = std::max(1, std::min(want, (dim + 511) / 512));
+    gemv_chunk = ((dim + gemv_chunks - 1) / gemv_chunks + 63) / 64 * 64;
+    gemv_chunks = (dim + gemv_chunk - 1) / gemv_chunk;
+    LUM_TRY(gemv_part_buf.alloc(sizeof(double2) * (size_t)gemv_chunks * dim));
+  }
+  const dim3 grid((dim + kGemvRows - 1) / kGemvRows, gemv_chunks);
   if (precision == LUM_FP32)
-    gemv_rows<float2><<<blocks, 256, 0, st>>>(dim, ld, A.as<float2>(), x, y, skip);
+    gemv_part<float2><<<grid, 32 * kGemvRows, 0, st>>>(dim, ld, gemv_chunk, A.as<float2>(), x,
+                                                       gemv_part_buf.as<double2>(), skip);
   else
-    gemv_rows<double2><<<blocks, 256, 0, st>>>(dim, ld, A.as<double2>(), x, y, skip);
+    gemv_part<double2><<<grid, 32 * kGemvRows, 0, st>>>(dim, ld, gemv_chunk, A.as<double2>(), x,
+                                                        gemv_part_buf.as<double2>(), skip);
+  LUM_CHECK_LAUNCH();
+  gemv_reduce<<<(dim + 255) / 256, 256, 0, st>>>(dim, gemv_chunks, gemv_part_buf.as<double2>(),
+                                                 y, skip);
   LUM_CHECK_LAUNCH();
   return LUM_OK;
 }

@@ -497,9 +497,21 @@ lum_status cgemm_tf32x3(CachedOperator& op, const double2* X, long long sxc, lon
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  // split K until the grid covers the SMs, keeping >= 16 stages per split
+  // Split K so that the grid fills whole waves of one CTA per SM: the
+  // smallest split whose last wave is >= 90 % full (else the fullest), each
+  // split keeping >= 16 stages.
+  const int kmax = std::max(1, std::min(16, ktiles / 16));
   int ksplit = 1;
-  if (mt * nt < sms) ksplit = std::min((sms + mt * nt - 1) / (mt * nt), std::max(1, ktiles / 16));
+  double best = 0.0;
+  for (int ks = 1; ks <= kmax; ++ks) {
+    const int ctas = mt * nt * ks;
+    const double eff = (double)ctas / ((double)sms * ((ctas + sms - 1) / sms));
+    if (eff > best + 1e-9) {
+      best = eff;
+      ksplit = ks;
+    }
+    if (eff >= 0.9) break;
+  }
   const int kps = (ktiles + ksplit - 1) / ksplit;
   ksplit = (ktiles + kps - 1) / kps;
 

@@ -192,8 +192,10 @@ struct CachedOperator {
   size_t ld = 0;            // row pitch in complex entries (dim rounded up to 16)
   int precision = LUM_FP32; // storage precision of A
   DevBuf A;                 // float2 or double2 [dim][ld] row-major, zero padding
-  DevBuf x32;               // float2[dim] staging for FP32 storage
   TcWork tc;
+  int gemv_chunks = 0;      // column chunks of the GEMV (0: not yet chosen)
+  int gemv_chunk = 0;       // complex entries per chunk
+  DevBuf gemv_part_buf;     // double2 [gemv_chunks][dim] per-chunk partial sums
   lum_status allocate(int dim, int precision);
   lum_status upload(const double* host, cudaStream_t st);
   lum_status assemble(const OtfOperator& geo, cudaStream_t st);
