@@ -295,7 +295,8 @@ lum_status batch_apply(const BatchGeom& g, int precision, const double2* x, doub
                        cudaStream_t st);                                             // otf.cu
 int batch_occupancy(const BatchGeom& g, int precision);                              // otf.cu
 
-const char* f32_variant_name(int v);  // otf.cu
+const char* f32_variant_name(int v);    // otf.cu
+const char* f32x2_variant_name(int v);  // otf.cu
 lum_status assemble_from_table(const OtfOperator& g, int precision, void* A, size_t ld,
                                cudaStream_t st);  // table.cu
 

@@ -251,6 +251,101 @@ otf_epilogue(int n, const double2* __restrict__ x, const double2* __restrict__ i
   }
 }
 
+// The epilogue of a two-vector application: the same sums for x and x2, with
+// each FCD correction tensor read once for both vectors.  A vector whose
+// skip flag is set is left untouched.
+template <typename TP, typename TC>
+__global__ void __launch_bounds__(256)
+otf_epilogue2(int n, const double2* __restrict__ x, const double2* __restrict__ x2,
+              const double2* __restrict__ inv_alpha, const TP* __restrict__ partial,
+              const TP* __restrict__ partial2, int nparts, int ell_w,
+              const int* __restrict__ near_j, const TC* __restrict__ fcd,
+              double2* __restrict__ y, double2* __restrict__ y2, const int* __restrict__ skip,
+              const int* __restrict__ skip2) {
+  const bool l1 = !(skip && *skip), l2 = !(skip2 && *skip2);  // grid-uniform
+  if (!l1 && !l2) return;
+  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = min(gid / kEpiTPR, n - 1);
+  const int sub = gid % kEpiTPR;
+  const bool live = gid / kEpiTPR < n;
+  double gr[3] = {0, 0, 0}, gi[3] = {0, 0, 0}, hr[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+  const size_t stride = 3 * (size_t)n;
+  for (int s = sub; s < nparts; s += kEpiTPR) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      if (l1) {
+        const double2 p = to_d2(partial[s * stride + 3 * i + a]);
+        gr[a] += p.x;
+        gi[a] += p.y;
+      }
+      if (l2) {
+        const double2 p = to_d2(partial2[s * stride + 3 * i + a]);
+        hr[a] += p.x;
+        hi[a] += p.y;
+      }
+    }
+  }
+  for (int w = sub; w < ell_w; w += kEpiTPR) {
+    const int j = near_j[(size_t)w * n + i];
+    if (j < 0) break;  // lists are packed: the rest of this row is padding
+    double2 xj[3], zj[3];
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      xj[b] = l1 ? x[3 * j + b] : make_double2(0.0, 0.0);
+      zj[b] = l2 ? x2[3 * j + b] : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        const double2 c = to_d2(fcd[((size_t)w * 9 + 3 * a + b) * n + i]);
+        gr[a] += c.x * xj[b].x - c.y * xj[b].y;
+        gi[a] += c.x * xj[b].y + c.y * xj[b].x;
+        hr[a] += c.x * zj[b].x - c.y * zj[b].y;
+        hi[a] += c.x * zj[b].y + c.y * zj[b].x;
+      }
+  }
+#pragma unroll
+  for (int o = 1; o < kEpiTPR; o <<= 1)
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      gr[a] += __shfl_xor_sync(0xffffffffu, gr[a], o);
+      gi[a] += __shfl_xor_sync(0xffffffffu, gi[a], o);
+      hr[a] += __shfl_xor_sync(0xffffffffu, hr[a], o);
+      hi[a] += __shfl_xor_sync(0xffffffffu, hi[a], o);
+    }
+  if (!live || sub != 0) return;
+  double2 m[9];
+#pragma unroll
+  for (int e = 0; e < 9; ++e) m[e] = inv_alpha[(size_t)e * n + i];
+  if (l1) {
+    const double2 xi[3] = {x[3 * i], x[3 * i + 1], x[3 * i + 2]};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      double sr = 0.0, si = 0.0;
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        sr += m[3 * a + b].x * xi[b].x - m[3 * a + b].y * xi[b].y;
+        si += m[3 * a + b].x * xi[b].y + m[3 * a + b].y * xi[b].x;
+      }
+      y[3 * i + a] = make_double2(sr - gr[a], si - gi[a]);
+    }
+  }
+  if (l2) {
+    const double2 zi[3] = {x2[3 * i], x2[3 * i + 1], x2[3 * i + 2]};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      double sr = 0.0, si = 0.0;
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        sr += m[3 * a + b].x * zi[b].x - m[3 * a + b].y * zi[b].y;
+        si += m[3 * a + b].x * zi[b].y + m[3 * a + b].y * zi[b].x;
+      }
+      y2[3 * i + a] = make_double2(sr - hr[a], si - hi[a]);
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Near-pair list (FCD).  The near test is the reference's, in FP64 without
 // contraction: dist = sqrt((dx*dx + dy*dy) + dz*dz); near = !(dist > 2*cell)
@@ -556,6 +651,7 @@ struct F32X2VariantEntry {
 const F32X2VariantEntry kF32X2Variants[] = {
     {"x2_rows2_minb4", 2, F32X2Variant<1, 4>::launch<false>, F32X2Variant<1, 4>::launch<true>, F32X2Variant<1, 4>::occupancy},
     {"x2_rows4_minb2", 4, F32X2Variant<2, 2>::launch<false>, F32X2Variant<2, 2>::launch<true>, F32X2Variant<2, 2>::occupancy},
+    {"x2_rows4_minb3", 4, F32X2Variant<2, 3>::launch<false>, F32X2Variant<2, 3>::launch<true>, F32X2Variant<2, 3>::occupancy},
 };
 constexpr int kNumF32X2Variants = sizeof(kF32X2Variants) / sizeof(kF32X2Variants[0]);
 std::map<std::tuple<int, int, int>, int> g_tune_x2_cache;
@@ -564,6 +660,10 @@ std::map<std::tuple<int, int, int>, int> g_tune_x2_cache;
 
 const char* f32_variant_name(int v) {
   return (v >= 0 && v < kNumF32Variants) ? kF32Variants[v].name : "none";
+}
+
+const char* f32x2_variant_name(int v) {
+  return (v >= 0 && v < kNumF32X2Variants) ? kF32X2Variants[v].name : "none";
 }
 
 lum_status OtfOperator::build_geometry(const double* pos_host, int n_, cudaStream_t st) {
@@ -1126,13 +1226,9 @@ lum_status OtfOperator::apply2(int precision, const double2* x, const double2* x
       LUM_CHECK_LAUNCH();
       nparts = 2 * ns;
     }
-    otf_epilogue<float2, float2><<<epi_blocks, 256, 0, st>>>(
-        n, x, inv_alpha.as<double2>(), part, nparts, ell_w, near_j.as<int>(), fcd32.as<float2>(),
-        y, skip);
-    LUM_CHECK_LAUNCH();
-    otf_epilogue<float2, float2><<<epi_blocks, 256, 0, st>>>(
-        n, x2, inv_alpha.as<double2>(), part2, nparts, ell_w, near_j.as<int>(),
-        fcd32.as<float2>(), y2, skip2);
+    otf_epilogue2<float2, float2><<<epi_blocks, 256, 0, st>>>(
+        n, x, x2, inv_alpha.as<double2>(), part, part2, nparts, ell_w, near_j.as<int>(),
+        fcd32.as<float2>(), y, y2, skip, skip2);
     LUM_CHECK_LAUNCH();
     return LUM_OK;
   }
@@ -1156,13 +1252,9 @@ lum_status OtfOperator::apply2(int precision, const double2* x, const double2* x
     LUM_CHECK_LAUNCH();
     nparts = 2 * ns;
   }
-  otf_epilogue<double2, double2><<<epi_blocks, 256, 0, st>>>(
-      n, x, inv_alpha.as<double2>(), part, nparts, ell_w, near_j.as<int>(), fcd64.as<double2>(),
-      y, skip);
-  LUM_CHECK_LAUNCH();
-  otf_epilogue<double2, double2><<<epi_blocks, 256, 0, st>>>(
-      n, x2, inv_alpha.as<double2>(), part2, nparts, ell_w, near_j.as<int>(),
-      fcd64.as<double2>(), y2, skip2);
+  otf_epilogue2<double2, double2><<<epi_blocks, 256, 0, st>>>(
+      n, x, x2, inv_alpha.as<double2>(), part, part2, nparts, ell_w, near_j.as<int>(),
+      fcd64.as<double2>(), y, y2, skip, skip2);
   LUM_CHECK_LAUNCH();
   return LUM_OK;
 }

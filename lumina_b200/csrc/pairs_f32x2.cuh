@@ -42,8 +42,7 @@ template <bool FAST, bool IMAGE, bool LOFREE, bool CHECKED, int RP, int NR>
 __device__ __forceinline__ void pair_tile_f32x2(
     const float4 (*__restrict__ sS)[kOtfBlock], int cnt, int jt, const int* irow,
     const float2* OX, const float2* OY, const float2* OZ, const float2* LX, const float2* LY,
-    const float2* LZ, float2 (*acc)[6], float2 (*acc2)[6], float k, float2 inv_k2, float2 s02,
-    float2 k2) {
+    const float2* LZ, float2 (*acc)[6], float2 (*acc2)[6], float2 kk2, float2 s02) {
 #pragma unroll 2
   for (int jj = 0; jj < cnt; ++jj) {
     const float4 S0 = sS[0][jj], S1 = sS[1][jj], S2 = sS[2][jj], S3 = sS[3][jj], S4 = sS[4][jj];
@@ -78,8 +77,9 @@ __device__ __forceinline__ void pair_tile_f32x2(
         if (sx) { r2.x = 1.0f; keep.x = 0.0f; }
         if (sy) { r2.y = 1.0f; keep.y = 0.0f; }
       }
-      const float2 ir = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
-      const float2 kR = mul2(mul2(r2, ir), k2);          // k R
+      const float2 kr2 = mul2(r2, kk2);                   // (k R)^2
+      const float2 u = make_float2(rsqrtf(kr2.x), rsqrtf(kr2.y));  // 1/(kR)
+      const float2 kR = mul2(kr2, u);                     // k R
       float2 sn, cs;
       if (FAST) {
         __sincosf(kR.x, &sn.x, &cs.x);
@@ -88,7 +88,6 @@ __device__ __forceinline__ void pair_tile_f32x2(
         sincosf(kR.x, &sn.x, &cs.x);
         sincosf(kR.y, &sn.y, &cs.y);
       }
-      const float2 u = mul2(ir, inv_k2);                 // 1/(kR)
       const float2 u2 = mul2(u, u);
       float2 q = mul2(s02, u);                           // k^3/(4 pi) u
       if (CHECKED) q = mul2(q, keep);
@@ -97,17 +96,20 @@ __device__ __forceinline__ void pair_tile_f32x2(
       // A = pf a,  a = 1 - u^2 + i u
       const float2 Ar = sub2(mul2(pr, ar), mul2(pi, u));
       const float2 Ai = fma2(pr, u, mul2(pi, ar));
-      // B' = pf b / R^2 with b = 3u^2 - 1 - 3iu = 2 - 3a, so B' = (2 pf - 3 A) ir^2
-      const float2 m3 = make_float2(-3.0f, -3.0f);
-      const float2 ir2 = mul2(ir, ir);
+      // B' = pf b / R^2 with b = 3u^2 - 1 - 3iu = 2 - 3a, so B' = (2 pf - 3 A) ir^2,
+      // ir^2 = u^2 k^2
+      const float2 m3 = make_float2(-3.0f, -3.0f), m1 = make_float2(-1.0f, -1.0f);
+      const float2 ir2 = mul2(u2, kk2);
       const float2 Br = mul2(fma2(Ar, m3, add2(pr, pr)), ir2);
       const float2 Bi = mul2(fma2(Ai, m3, add2(pi, pi)), ir2);
+      // -Ai and -Bi turn the real parts of the complex products into one FMA
+      // each (shared by every right-hand side)
+      const float2 nAi = mul2(Ai, m1), nBi = mul2(Bi, m1);
       // d . x_j
       const float2 dxr = fma2(dx, x0r, fma2(dy, x1r, mul2(dz, x2r)));
       const float2 dxi = fma2(dx, x0i, fma2(dy, x1i, mul2(dz, x2i)));
-      const float2 tr = sub2(mul2(Br, dxr), mul2(Bi, dxi));
+      const float2 tr = fma2(Br, dxr, mul2(nBi, dxi));
       const float2 ti = fma2(Br, dxi, mul2(Bi, dxr));
-      const float2 nAi = mul2(Ai, make_float2(-1.0f, -1.0f));
       acc[p][0] = fma2(tr, dx, fma2(Ar, x0r, fma2(nAi, x0i, acc[p][0])));
       acc[p][1] = fma2(ti, dx, fma2(Ar, x0i, fma2(Ai, x0r, acc[p][1])));
       acc[p][2] = fma2(tr, dy, fma2(Ar, x1r, fma2(nAi, x1i, acc[p][2])));
@@ -117,7 +119,7 @@ __device__ __forceinline__ void pair_tile_f32x2(
       if constexpr (NR == 2) {
         const float2 dyr = fma2(dx, y0r, fma2(dy, y1r, mul2(dz, y2r)));
         const float2 dyi = fma2(dx, y0i, fma2(dy, y1i, mul2(dz, y2i)));
-        const float2 ur = sub2(mul2(Br, dyr), mul2(Bi, dyi));
+        const float2 ur = fma2(Br, dyr, mul2(nBi, dyi));
         const float2 ui = fma2(Br, dyi, mul2(Bi, dyr));
         acc2[p][0] = fma2(ur, dx, fma2(Ar, y0r, fma2(nAi, y0i, acc2[p][0])));
         acc2[p][1] = fma2(ui, dx, fma2(Ar, y0i, fma2(Ai, y0r, acc2[p][1])));
@@ -172,7 +174,7 @@ __device__ __forceinline__ void pairs_f32_cta(
       for (int c = 0; c < 6; ++c) acc2[p][c] = f2(0.f, 0.f);
     }
   }
-  const float2 inv_k2 = f2(inv_k, inv_k), s02 = f2(s0, s0), k2 = f2(k, k);
+  const float2 kk2 = f2(k * k, k * k), s02 = f2(s0, s0);
   const int row_end = row0 + kOtfBlock * ROWS;
   // Software pipeline: the source of the next tile is loaded into registers
   // before the current tile is computed, hiding its global-load latency.
@@ -241,10 +243,10 @@ __device__ __forceinline__ void pairs_f32_cta(
     const bool diag = IMAGE || (jt < row_end && jt + kOtfBlock > row0);  // CTA-uniform
     if (diag)
       pair_tile_f32x2<FAST, IMAGE, LOFREE, true, RP, NR>(sS, cnt, jt, irow, OX, OY, OZ, LX, LY,
-                                                         LZ, acc, acc2, k, inv_k2, s02, k2);
+                                                         LZ, acc, acc2, kk2, s02);
     else
       pair_tile_f32x2<FAST, IMAGE, LOFREE, false, RP, NR>(sS, cnt, jt, irow, OX, OY, OZ, LX, LY,
-                                                          LZ, acc, acc2, k, inv_k2, s02, k2);
+                                                          LZ, acc, acc2, kk2, s02);
   }
 #pragma unroll
   for (int p = 0; p < RP; ++p) {
