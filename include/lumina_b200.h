@@ -259,6 +259,36 @@ LUM_API int lum_solve_gmres_multi_device(lum_session* s, int nrhs, const void* b
                                          void* x_dev, double tol, int max_iter, int restart,
                                          int mode, lum_solve_info* info, void* stream);
 
+/* ---- fields from solved moments (fields.rs) ------------------------------- */
+/* field_at_point (crates/lumina-core/src/fields.rs:18-49) at m observation
+ * points obs (3m doubles): E = E_inc + sum_i G(r - r_i) p_i, the point-dipole
+ * tensor of greens.rs:34-71, dipoles with |r - r_i|^2 < 1e-20 skipped, FP64.
+ * moments: 3N complex (the solved p).  The incident field is
+ * IncidentField::at_position (types.rs:60-73) with a real polarisation.
+ * field (3m complex) and intensity (|E|^2, m doubles) may each be NULL.
+ * n = 0 gives the incident field. */
+LUM_API int lum_near_field(lum_ctx* ctx, int n_dipoles, const double* pos, const double* moments,
+                           double k, const double direction[3], const double polarisation[3],
+                           double amplitude, int n_obs, const double* obs, double* field,
+                           double* intensity);
+/* compute_near_field_map (fields.rs:52-105, plane_basis :111-139): the
+ * nx x ny grid on the plane (centre, normal, half_width, half_height), row
+ * iy outer and column ix inner, its |E|^2 and extent [x_min, x_max, y_min,
+ * y_max].  positions: 3*nx*ny doubles (may be NULL), intensity: nx*ny. */
+LUM_API int lum_near_field_map(lum_ctx* ctx, int n_dipoles, const double* pos,
+                               const double* moments, double k, const double direction[3],
+                               const double polarisation[3], double amplitude,
+                               const double centre[3], const double normal[3], double half_width,
+                               double half_height, int nx, int ny, double* positions,
+                               double* intensity, double extent[4]);
+/* compute_far_field (fields.rs:147-221): n_theta x n_phi directions,
+ * theta = pi it / max(n_theta - 1, 1), phi = 2 pi ip / n_phi (it outer);
+ * intensity |(I - r r) . F|^2 with F = sum_i p_i exp(-i k r . r_i), FP64.
+ * theta, phi and intensity hold n_theta * n_phi doubles each. */
+LUM_API int lum_far_field(lum_ctx* ctx, int n_dipoles, const double* pos, const double* moments,
+                          double k, int n_theta, int n_phi, double* theta, double* phi,
+                          double* intensity);
+
 /* ---- measurement --------------------------------------------------------- */
 /* While enabled, every launch of the session's dominant matvec kernel (the
  * dense pair kernel, or the GEMV of a cached session) is bracketed by CUDA

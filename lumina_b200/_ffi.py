@@ -98,6 +98,13 @@ SIGNATURES = {
                                   POINTER(c_int)]),
     "lum_session_kernel_config": (c_int, [c_void_p, c_char_p, c_size_t]),
     "lum_measure_fma_peak": (c_int, [c_void_p, POINTER(c_double), POINTER(c_double)]),
+    "lum_near_field": (c_int, [c_void_p, c_int, _dp, _dp, c_double, _dp, _dp, c_double, c_int,
+                               _dp, c_void_p, c_void_p]),
+    "lum_near_field_map": (c_int, [c_void_p, c_int, _dp, _dp, c_double, _dp, _dp, c_double,
+                                   _dp, _dp, c_double, c_double, c_int, c_int, c_void_p, _dp,
+                                   _dp]),
+    "lum_far_field": (c_int, [c_void_p, c_int, _dp, _dp, c_double, c_int, c_int, _dp, _dp,
+                              _dp]),
     "lum_matvec_onthefly_noalloc": (c_int, [c_int, c_void_p, c_void_p, c_double, c_void_p,
                                             c_void_p, c_void_p]),
     "lum_batch_create": (c_int, [c_void_p, c_int, POINTER(c_int), _dp, _dp, _dp, _dp, c_int,

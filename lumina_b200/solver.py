@@ -106,6 +106,21 @@ class CdaSolver:
         return self.cross_sections_from_response(dipoles, resp, params)
 
 
+    def compute_near_field(self, dipoles: DipoleSet, response: DipoleResponse, plane):
+        """OpticalSolver::compute_near_field (cda/mod.rs:421-430)."""
+        from .fields import compute_near_field_map
+        k = wavenumber(response.wavelength_nm, response.environment_n)
+        return compute_near_field_map(self.backend, dipoles.positions, response.moments, plane,
+                                      k, self.incident_field)
+
+    def compute_far_field(self, dipoles: DipoleSet, response: DipoleResponse, n_theta: int,
+                          n_phi: int):
+        """OpticalSolver::compute_far_field (cda/mod.rs:432-441)."""
+        from .fields import compute_far_field
+        k = wavenumber(response.wavelength_nm, response.environment_n)
+        return compute_far_field(self.backend, dipoles.positions, response, k, n_theta, n_phi)
+
+
 def circular_dichroism(response_x: DipoleResponse, response_y: DipoleResponse, k: float) -> float:
     """k * sum_i [Im p_y^(x) - Im p_x^(y)]  (fields.rs:236-253)."""
     return float(k * np.sum(response_x.moments[:, 1].imag - response_y.moments[:, 0].imag))

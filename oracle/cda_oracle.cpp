@@ -1247,6 +1247,111 @@ double orc_circular_dichroism(int n, const double* mom_x, const double* mom_y, d
   return k * delta;
 }
 
+// ---------------------------------------------------------------------------
+// Fields from solved moments, fields.rs.
+// ---------------------------------------------------------------------------
+// field_at_point, fields.rs:18-49: the incident field at the point, then, in
+// dipole order, G(r_obs, r_i) . p_i for every dipole with r^2 >= 1e-20.
+// moments are 3N complex; out is 3M complex.
+void orc_field_at_points(int n, const double* pos, const double* moments, double k,
+                         const double* dir, const double* pol, double amplitude, int m,
+                         const double* obs, double* out) {
+#pragma omp parallel for schedule(static)
+  for (int q = 0; q < m; ++q) {
+    const double* o = obs + 3 * (size_t)q;
+    double einc[6];
+    orc_incident_field(1, o, dir, pol, amplitude, k, einc);
+    C e[3] = {C{einc[0], einc[1]}, C{einc[2], einc[3]}, C{einc[4], einc[5]}};
+    for (int i = 0; i < n; ++i) {
+      const double* r = pos + 3 * (size_t)i;
+      double dx = o[0] - r[0], dy = o[1] - r[1], dz = o[2] - r[2];
+      double r_sq = dx * dx + dy * dy + dz * dz;
+      if (r_sq < 1e-20) continue;
+      T3 g;
+      if (!greens(o, r, k, g)) continue;
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+          const size_t at = 2 * (3 * (size_t)i + b);
+          e[a] = add(e[a], mul(g[a][b], C{moments[at], moments[at + 1]}));
+        }
+    }
+    for (int a = 0; a < 3; ++a) {
+      out[2 * (3 * (size_t)q + a)] = e[a].re;
+      out[2 * (3 * (size_t)q + a) + 1] = e[a].im;
+    }
+  }
+}
+
+// plane_basis + the grid of compute_near_field_map, fields.rs:52-139.
+// positions: 3*nx*ny doubles (iy outer, ix inner); extent[4].
+void orc_near_field_plane(const double* centre, const double* normal, double half_width,
+                          double half_height, int nx, int ny, double* positions,
+                          double* extent) {
+  const double nl = std::sqrt(normal[0] * normal[0] + normal[1] * normal[1] +
+                              normal[2] * normal[2]);
+  const double n[3] = {normal[0] / nl, normal[1] / nl, normal[2] / nl};
+  double seed[3] = {0.0, 1.0, 0.0};
+  if (std::fabs(n[0]) < 0.9) {
+    seed[0] = 1.0;
+    seed[1] = 0.0;
+  }
+  const double dot = seed[0] * n[0] + seed[1] * n[1] + seed[2] * n[2];
+  const double ur[3] = {seed[0] - dot * n[0], seed[1] - dot * n[1], seed[2] - dot * n[2]};
+  const double ul = std::sqrt(ur[0] * ur[0] + ur[1] * ur[1] + ur[2] * ur[2]);
+  const double u[3] = {ur[0] / ul, ur[1] / ul, ur[2] / ul};
+  const double v[3] = {n[1] * u[2] - n[2] * u[1], n[2] * u[0] - n[0] * u[2],
+                       n[0] * u[1] - n[1] * u[0]};
+  const double x_min = -half_width, x_max = half_width;
+  const double y_min = -half_height, y_max = half_height;
+  const double dx = nx > 1 ? (x_max - x_min) / (double)(nx - 1) : 0.0;
+  const double dy = ny > 1 ? (y_max - y_min) / (double)(ny - 1) : 0.0;
+  size_t q = 0;
+  for (int iy = 0; iy < ny; ++iy)
+    for (int ix = 0; ix < nx; ++ix) {
+      const double uu = x_min + (double)ix * dx;
+      const double vv = y_min + (double)iy * dy;
+      for (int c = 0; c < 3; ++c) positions[3 * q + c] = centre[c] + uu * u[c] + vv * v[c];
+      ++q;
+    }
+  extent[0] = centre[0] + x_min * u[0] + y_min * v[0];
+  extent[1] = centre[0] + x_max * u[0] + y_max * v[0];
+  extent[2] = centre[1] + x_min * u[1] + y_min * v[1];
+  extent[3] = centre[1] + x_max * u[1] + y_max * v[1];
+}
+
+// compute_far_field, fields.rs:147-221: intensity |(I - rr) . F|^2 with
+// F = sum_i p_i exp(-i k r.r_i), theta = pi it/max(nt-1,1), phi = 2 pi ip/np.
+void orc_far_field(int n, const double* pos, const double* moments, double k, int n_theta,
+                   int n_phi, double* theta, double* phi, double* intensity) {
+#pragma omp parallel for schedule(static)
+  for (int it = 0; it < n_theta; ++it) {
+    const double th = PI * (double)it / (double)std::max(n_theta - 1, 1);
+    const double sin_t = std::sin(th), cos_t = std::cos(th);
+    for (int ip = 0; ip < n_phi; ++ip) {
+      const double ph = 2.0 * PI * (double)ip / (double)n_phi;
+      const double sin_p = std::sin(ph), cos_p = std::cos(ph);
+      const double rh[3] = {sin_t * cos_p, sin_t * sin_p, cos_t};
+      C f[3] = {cc(0.0), cc(0.0), cc(0.0)};
+      for (int i = 0; i < n; ++i) {
+        const double* r = pos + 3 * (size_t)i;
+        const double kdotr = k * (rh[0] * r[0] + rh[1] * r[1] + rh[2] * r[2]);
+        const C phase = cexp(C{0.0, -kdotr});
+        for (int a = 0; a < 3; ++a) {
+          const size_t at = 2 * (3 * (size_t)i + a);
+          f[a] = add(f[a], mul(C{moments[at], moments[at + 1]}, phase));
+        }
+      }
+      const C rdotf = add(add(muls(f[0], rh[0]), muls(f[1], rh[1])), muls(f[2], rh[2]));
+      double inten = 0.0;
+      for (int a = 0; a < 3; ++a) inten += norm_sqr(sub(f[a], muls(rdotf, rh[a])));
+      const size_t q = (size_t)it * n_phi + ip;
+      theta[q] = th;
+      phi[q] = ph;
+      intensity[q] = inten;
+    }
+  }
+}
+
 // The reference's WGSL shaders, restated in FP32 (the "reference GPU
 // equivalent" of the cached path).  matrix_assemble.wgsl:21-103 and
 // matvec.wgsl:19-39; the host diagonal patch is gpu.rs:585-603.

@@ -55,6 +55,10 @@ def _load():
         "orc_greens_filtered": (c_int, [_dp, _dp, c_double, c_double, _dp]),
         "orc_invert_3x3": (c_int, [_dp, _dp]),
         "orc_incident_field": (None, [c_int, _dp, _dp, _dp, c_double, c_double, _dp]),
+        "orc_field_at_points": (None, [c_int, _dp, _dp, c_double, _dp, _dp, c_double, c_int,
+                                       _dp, _dp]),
+        "orc_near_field_plane": (None, [_dp, _dp, c_double, c_double, c_int, c_int, _dp, _dp]),
+        "orc_far_field": (None, [c_int, _dp, _dp, c_double, c_int, c_int, _dp, _dp, _dp]),
         "orc_ewald_evaluate": (None, [ctypes.c_void_p, _dp, _dp, c_double, c_int, _dp]),
         "orc_lattice_eta": (c_double, [ctypes.c_void_p]),
         "orc_erfc": (c_double, [c_double]),
@@ -346,6 +350,39 @@ def spline(xs, ys):
         return lib().orc_spline_eval(len(xs), _p(xs), _p(ys), _p(y2), float(x))
 
     return ev
+
+
+def field_at_points(pos, moments, k, obs, direction=(0, 0, 1), polarisation=(1, 0, 0),
+                    amplitude=1.0):
+    """fields.rs:18-49 at every row of obs: (M, 3) complex."""
+    pos = _vec(pos).reshape(-1, 3)
+    obs = _vec(obs).reshape(-1, 3)
+    mom = np.ascontiguousarray(np.asarray(moments, np.complex128).reshape(-1))
+    out = np.zeros(3 * obs.shape[0], np.complex128)
+    lib().orc_field_at_points(pos.shape[0], _p(pos), _p(mom.view(np.float64)), k,
+                              _p(_vec(direction)), _p(_vec(polarisation)), amplitude,
+                              obs.shape[0], _p(obs), _p(out.view(np.float64)))
+    return out.reshape(-1, 3)
+
+
+def near_field_plane(centre, normal, half_width, half_height, nx, ny):
+    """Grid of compute_near_field_map (fields.rs:52-139): positions (nx*ny, 3), extent."""
+    pos = np.zeros(3 * nx * ny)
+    ext = np.zeros(4)
+    lib().orc_near_field_plane(_p(_vec(centre)), _p(_vec(normal)), half_width, half_height,
+                               nx, ny, _p(pos), _p(ext))
+    return pos.reshape(-1, 3), ext
+
+
+def far_field(pos, moments, k, n_theta, n_phi):
+    """compute_far_field (fields.rs:147-221): theta, phi, intensity (n_theta*n_phi)."""
+    pos = _vec(pos).reshape(-1, 3)
+    mom = np.ascontiguousarray(np.asarray(moments, np.complex128).reshape(-1))
+    m = n_theta * n_phi
+    th, ph, it = np.zeros(m), np.zeros(m), np.zeros(m)
+    lib().orc_far_field(pos.shape[0], _p(pos), _p(mom.view(np.float64)), k, n_theta, n_phi,
+                        _p(th), _p(ph), _p(it))
+    return th, ph, it
 
 
 def circular_dichroism(mom_x, mom_y, k):
