@@ -56,12 +56,14 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--workload", default="cuboid",
-                   choices=["cuboid", "clusters", "dimer", "metasurface", "cached", "fields"],
+                   choices=["cuboid", "clusters", "dimer", "metasurface", "cached", "fields",
+                            "fft"],
                    help="cuboid: the headline N=30k solve; clusters: 256 Drude ellipsoids x 2 "
                         "polarisations in one batch; dimer: helix-dimer adjoint gradients; "
                         "metasurface: periodic Ewald + substrate sweep; cached: the assembled "
                         "3N x 3N matrix, single-vector GEMV and multi-RHS tensor-core product; "
-                        "fields: near-field map and far field from solved moments")
+                        "fields: near-field map and far field from solved moments; fft: the "
+                        "headline cuboid through the block-Toeplitz FFT operator")
     p.add_argument("--nrhs", type=int, default=128, help="right-hand sides (cached workload)")
     p.add_argument("--clusters", type=int, default=256)
     p.add_argument("--spacing", type=float, default=None)
@@ -456,6 +458,8 @@ def run_secondary(args):
             line = _bench_dimer(args, bk, stream, torch, lb, configs)
         elif args.workload == "cached":
             line = _bench_cached(args, bk, stream, torch, lb, configs)
+        elif args.workload == "fft":
+            line = _bench_fft(args, bk, stream, torch, lb, configs)
         elif args.workload == "fields":
             line = _bench_fields(args, bk, stream, torch, lb, configs, fp64_peak)
         else:
@@ -693,6 +697,74 @@ def _bench_cached(args, bk, stream, torch, lb, configs):
                 "rel_diff_vs_cuda_cores": err,
                 "gemv_equivalent_ms": ms_gemv * R},
             "e2e": None}
+
+
+def _bench_fft(args, bk, stream, torch, lb, configs):
+    """The headline cuboid (60x50x10 nm, N = 30,000, FCD cell 1 nm, tol 1e-8,
+    520/650/800 nm) solved through the block-Toeplitz FFT operator
+    (fft_matvec.rs, widened to FCD): FP32+refine and plain FP64 solves, C_ext
+    against the on-the-fly FP64 solve, and the time of one operator
+    application in each precision."""
+    lams = [float(v) for v in args.wavelengths.split(",")]
+    base, per = build_inputs(args, lams)
+    n = base.n
+    inv = [lb.invert_polarisability(w.alpha) for w in per]
+    rhs = [lb.incident_field(w.positions, w.k, lb.IncidentField()) for w in per]
+    F = bk.create_fft_session(base.positions, inv[0], per[0].k, True, 1.0)
+    F.set_stream(stream.cuda_stream)
+    flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")
+    b_dev = [torch.from_numpy(r).to("cuda") for r in rhs]
+    x_dev = torch.zeros(3 * n, dtype=torch.complex128, device="cuda")
+    rows, t32, t64 = [], 0.0, 0.0
+    for i, lam in enumerate(lams):
+        F.set_wavelength(per[i].k, inv[i])
+        for _ in range(args.warmup):
+            F.solve_device(b_dev[i].data_ptr(), x_dev.data_ptr(), args.tol, args.max_iter, 30,
+                           "fp32_refine", stream.cuda_stream)
+        flush.zero_()
+        info32, ms32 = _timed(stream, lambda: F.solve_device(
+            b_dev[i].data_ptr(), x_dev.data_ptr(), args.tol, args.max_iter, 30, "fp32_refine",
+            stream.cuda_stream))
+        x32 = x_dev.cpu().numpy()
+        flush.zero_()
+        info64, ms64 = _timed(stream, lambda: F.solve_device(
+            b_dev[i].data_ptr(), x_dev.data_ptr(), args.tol, args.max_iter, 30, "fp64",
+            stream.cuda_stream))
+        x64 = x_dev.cpu().numpy()
+        c32 = lb.cross_sections(base.positions, inv[i], x32, per[i].k, lb.IncidentField())
+        c64 = lb.cross_sections(base.positions, inv[i], x64, per[i].k, lb.IncidentField())
+        # the on-the-fly FP64 operator's C_ext at this wavelength (reference semantics)
+        with bk.create_onthefly_session(base.positions, inv[i], per[i].k, True, 1.0) as O:
+            xo, _ = O.solve(rhs[i], args.tol, args.max_iter, 30, "fp64")
+        co = lb.cross_sections(base.positions, inv[i], xo, per[i].k, lb.IncidentField())
+        t32 += ms32
+        t64 += ms64
+        rows.append({"wavelength_nm": lam, "ms_fp32_refine": ms32, "ms_fp64": ms64,
+                     "iterations": info32["iterations"], "iterations_fp64": info64["iterations"],
+                     "cext_fft_fp32_refine": c32[0], "cext_onthefly_fp64": co[0],
+                     "cext_rel_err_vs_onthefly": abs(c32[0] - co[0]) / abs(co[0]),
+                     "cext_rel_err_fp64": abs(c64[0] - co[0]) / abs(co[0])})
+    xr = torch.randn(3 * n, dtype=torch.complex128, device="cuda")
+    yr = torch.empty_like(xr)
+    apply_ms = {}
+    for prec in ("fp32", "fp64"):
+        for _ in range(3):
+            F.matvec_device(xr.data_ptr(), yr.data_ptr(), prec, stream.cuda_stream)
+        _, ms = _timed(stream, lambda: [F.matvec_device(xr.data_ptr(), yr.data_ptr(), prec,
+                                                        stream.cuda_stream) for _ in range(20)])
+        apply_ms[prec] = ms / 20
+    cfg = F.kernel_config()
+    F.close()
+    nl = len(rows)
+    return {"metric": "dipole-solves/s at N=30k through the FFT (block-Toeplitz) operator, "
+                      "FP32+refine", "value": n * nl / (t32 * 1e-3), "unit": UNIT,
+            "higher_is_better": True, "steps": nl, "ms_per_step": t32 / nl, "scaling": "weak",
+            "dtype": "f32+f64", "mode": "fp32_refine",
+            "config": dict(workload_config(args, n), operator="fft (circulant 128x128x32)"),
+            "fp64_plain": {"value": n * nl / (t64 * 1e-3), "speedup_same_solves": t64 / t32},
+            "apply_ms": apply_ms,
+            "max_cext_rel_err_vs_onthefly_fp64": max(r["cext_rel_err_vs_onthefly"] for r in rows),
+            "per_wavelength": rows, "kernel_config": cfg, "e2e": None}
 
 
 def _bench_fields(args, bk, stream, torch, lb, configs, fp64_peak):

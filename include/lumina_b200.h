@@ -143,6 +143,19 @@ LUM_API int lum_session_create_onthefly(lum_ctx* ctx, int n_dipoles, const doubl
                                 double cell_size, const lum_lattice* lattice,
                                 const double k_bloch[3], const lum_substrate* substrate,
                                 lum_session** out);
+/* The reference's FftMatvecPlan (crates/lumina-core/src/solver/cda/
+ * fft_matvec.rs:77-258, chosen at cda/mod.rs:286-298) as a session: A x by a
+ * circulant-embedded 3D FFT convolution, O(N log N), FP64 or FP32.  Widened
+ * to FCD (the filtered tensor is a function of the displacement too, so the
+ * product equals the on-the-fly FCD operator) and to any set of nodes of a
+ * cubic lattice (empty nodes hold zero), not only a full box.  `spacing` is
+ * the lattice pitch (<= 0: cell_size, as detect_regular_grid takes it,
+ * fft_matvec.rs:19); every dipole must lie within 1e-6 spacing of a node,
+ * at most 512 nodes per axis, no lattice sum, no substrate.  The session
+ * supports matvec, the solves and set_wavelength. */
+LUM_API int lum_session_create_fft(lum_ctx* ctx, int n_dipoles, const double* pos,
+                                   const double* inv_alpha, double k, int use_fcd,
+                                   double cell_size, double spacing, lum_session** out);
 /* Re-targets an on-the-fly session to a new wavelength (k, alpha^-1,
  * substrate factor) keeping the geometry and near-pair list (the runner's
  * per-wavelength loop, runner.rs:150-183). */

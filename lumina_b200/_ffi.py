@@ -80,6 +80,8 @@ SIGNATURES = {
                                             c_double, c_void_p, _dp, c_void_p,
                                             POINTER(c_void_p)]),
     "lum_session_set_wavelength": (c_int, [c_void_p, c_double, _dp, c_void_p]),
+    "lum_session_create_fft": (c_int, [c_void_p, c_int, _dp, _dp, c_double, c_int, c_double,
+                                       c_double, POINTER(c_void_p)]),
     "lum_session_matvec": (c_int, [c_void_p, c_int, _dp, _dp]),
     "lum_session_matvec_device": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
     "lum_session_matmul_device": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),

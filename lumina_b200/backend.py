@@ -531,6 +531,19 @@ class CudaBackend:
                                               byref(h)), "assemble")
         return CudaSession(h, 3 * n, "cached", self)
 
+    def create_fft_session(self, positions, inv_alpha, k: float, use_fcd=True,
+                           cell_size=3.0, spacing=0.0) -> CudaSession:
+        """Block-Toeplitz session through 3D FFTs (fft_matvec.rs:77-258, widened
+        to FCD and to any set of cubic-lattice nodes)."""
+        pos = np.ascontiguousarray(np.asarray(positions, np.float64).reshape(-1, 3))
+        n = pos.shape[0]
+        ia = _c128(inv_alpha, 9 * n)
+        h = c_void_p()
+        _raise(self._lib.lum_session_create_fft(self._h, n, _dp(pos), _dp(ia.view(np.float64)),
+                                                float(k), int(bool(use_fcd)), float(cell_size),
+                                                float(spacing), byref(h)), "create_fft_session")
+        return CudaSession(h, 3 * n, "fft", self)
+
     def create_onthefly_session(self, positions, inv_alpha, k: float, use_fcd=True,
                                 cell_size=3.0, lattice=None, k_bloch=(0.0, 0.0, 0.0),
                                 substrate=None) -> CudaSession:

@@ -92,6 +92,7 @@ lum_status lum_session::apply(int precision, const double2* x, double2* y, const
     e1 = r.b;
   }
   if (kind == 0) return otf.apply(precision, x, y, stream, e0, e1, skip);
+  if (kind == 2) return fft.apply(precision, x, y, stream, e0, e1, skip);
   // cached session
   if (precision == LUM_FP64 && cached.precision == LUM_FP32 && otf.inv_alpha.p)
     return otf.apply(LUM_FP64, x, y, stream, nullptr, nullptr, skip);
@@ -412,6 +413,15 @@ int lum_session_create_onthefly(lum_ctx* ctx, int n, const double* pos, const do
 int lum_session_set_wavelength(lum_session* s, double k, const double* inv_alpha,
                                const lum_substrate* substrate) {
   if (bad_ptr(s, "session")) return LUM_ERR_INVALID;
+  if (s->kind == 2) {
+    if (substrate) {
+      set_error("the FFT operator has no substrate term");
+      return LUM_ERR_INVALID;
+    }
+    LUM_TRY(check_physics(s->n_dipoles, inv_alpha, k));
+    cudaSetDevice(s->ctx->device);
+    return s->fft.set_physics(k, inv_alpha, s->stream);
+  }
   if (!s->otf.inv_alpha.p) {
     set_error("set_wavelength needs a geometry session");
     return LUM_ERR_INVALID;
@@ -422,6 +432,24 @@ int lum_session_set_wavelength(lum_session* s, double k, const double* inv_alpha
                              substrate, s->stream));
   if (s->kind == 1) LUM_TRY(s->cached.assemble(s->otf, s->stream));
   LUM_TRY_CUDA(cudaStreamSynchronize(s->stream));
+  return LUM_OK;
+}
+
+int lum_session_create_fft(lum_ctx* ctx, int n, const double* pos, const double* inv_alpha,
+                           double k, int use_fcd, double cell, double spacing,
+                           lum_session** out) {
+  if (bad_ptr(ctx, "ctx") || bad_ptr(out, "out")) return LUM_ERR_INVALID;
+  *out = nullptr;
+  LUM_TRY(check_inputs(n, pos, inv_alpha, k));
+  lum_session* s = nullptr;
+  LUM_TRY(new_session(ctx, 2, 3 * n, &s));
+  lum_status st = s->fft.build(pos, n, spacing, cell, use_fcd, s->stream);
+  if (st == LUM_OK) st = s->fft.set_physics(k, inv_alpha, s->stream);
+  if (st != LUM_OK) {
+    lum_session_destroy(s);
+    return st;
+  }
+  *out = s;
   return LUM_OK;
 }
 
@@ -682,7 +710,8 @@ int lum_session_kernel_config(lum_session* s, char* buf, size_t len) {
   snprintf(buf, len,
            "kind=%s f32_variant=%s tuned_ms=%.4f nsplit32=%d nsplit64=%d ell_w=%d lofree=%d "
            "fast_trig=%d f32x2_variant=%s tuned_x2_ms=%.4f nsplit_x2=%d",
-           s->kind == 0 ? "onthefly" : "cached", lum::f32_variant_name(o.f32_variant),
+           s->kind == 0 ? "onthefly" : (s->kind == 1 ? "cached" : "fft"),
+           lum::f32_variant_name(o.f32_variant),
            (double)o.tuned_ms, o.nsplit32, o.nsplit64, o.ell_w, o.lofree, o.fast_trig,
            lum::f32x2_variant_name(o.f32x2_variant), (double)o.tuned_x2_ms, o.nsplit_x2);
   return LUM_OK;

@@ -214,6 +214,28 @@ lum_status cgemm_tf32x3(CachedOperator& op, const double2* X, long long sxc, lon
 // clears the record); synchronises `st`.
 lum_status cgemm_status(CachedOperator& op, cudaStream_t st);
 
+// --- block-Toeplitz operator through 3D FFTs (fft.cu) -----------------------
+struct FftOperator {
+  int n = 0;                // dipoles
+  int gn[3] = {1, 1, 1};    // lattice nodes per axis (bounding box of the dipoles)
+  int M[3] = {1, 1, 1};     // circulant dimensions: powers of two >= 2 gn - 1
+  size_t mtot = 1;          // M[0] M[1] M[2]
+  double spacing = 0.0, cell = 0.0, k = 0.0;
+  int use_fcd = 0;
+  size_t tw_off[3] = {0, 0, 0};
+  DevBuf d_node_dip;        // int [mtot]: dipole on each node, -1 if none
+  DevBuf d_grid_of;         // int [n]: node of each dipole
+  DevBuf inv_alpha;         // double2 [9][n]
+  DevBuf kern64, kern32;    // kernel spectra: 6 components (xx xy xz yy yz zz) x mtot
+  DevBuf buf64, buf32;      // 3 vector components x mtot
+  DevBuf tw64, tw32;        // twiddles exp(-2 pi i q / M[c]), q < M[c]/2, per axis
+  lum_status build(const double* pos_host, int n, double spacing, double cell, int use_fcd,
+                   cudaStream_t st);
+  lum_status set_physics(double k, const double* inv_alpha_host, cudaStream_t st);
+  lum_status apply(int precision, const double2* x, double2* y, cudaStream_t st,
+                   cudaEvent_t ev0, cudaEvent_t ev1, const int* skip);
+};
+
 // --- GMRES workspace --------------------------------------------------------
 struct GmresState {
   double2 H[(kMaxRestart + 1) * kMaxRestart];
@@ -316,13 +338,14 @@ struct lum_ctx {
 
 struct lum_session {
   lum_ctx* ctx = nullptr;
-  int kind = 0;                 // 0 on-the-fly, 1 cached
+  int kind = 0;                 // 0 on-the-fly, 1 cached, 2 FFT (lattice)
   int n_dipoles = 0;
   int dim = 0;                  // 3N
   cudaStream_t stream = nullptr;
   bool own_stream = true;
   lum::OtfOperator otf;
   lum::CachedOperator cached;
+  lum::FftOperator fft;
   lum::GmresWork gw;
   lum::DevBuf xbuf, ybuf, bbuf; // host-path staging
   // profiling of the dominant kernel
