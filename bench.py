@@ -57,13 +57,14 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--workload", default="cuboid",
                    choices=["cuboid", "clusters", "dimer", "metasurface", "cached", "fields",
-                            "fft"],
+                            "fft", "directions"],
                    help="cuboid: the headline N=30k solve; clusters: 256 Drude ellipsoids x 2 "
                         "polarisations in one batch; dimer: helix-dimer adjoint gradients; "
                         "metasurface: periodic Ewald + substrate sweep; cached: the assembled "
                         "3N x 3N matrix, single-vector GEMV and multi-RHS tensor-core product; "
                         "fields: near-field map and far field from solved moments; fft: the "
-                        "headline cuboid through the block-Toeplitz FFT operator")
+                        "headline cuboid through the block-Toeplitz FFT operator; directions: "
+                        "many incidence directions of one cached matrix on the tensor cores")
     p.add_argument("--nrhs", type=int, default=128, help="right-hand sides (cached workload)")
     p.add_argument("--clusters", type=int, default=256)
     p.add_argument("--spacing", type=float, default=None)
@@ -458,6 +459,8 @@ def run_secondary(args):
             line = _bench_dimer(args, bk, stream, torch, lb, configs)
         elif args.workload == "cached":
             line = _bench_cached(args, bk, stream, torch, lb, configs)
+        elif args.workload == "directions":
+            line = _bench_directions(args, bk, stream, torch, lb, configs)
         elif args.workload == "fft":
             line = _bench_fft(args, bk, stream, torch, lb, configs)
         elif args.workload == "fields":
@@ -697,6 +700,87 @@ def _bench_cached(args, bk, stream, torch, lb, configs):
                 "rel_diff_vs_cuda_cores": err,
                 "gemv_equivalent_ms": ms_gemv * R},
             "e2e": None}
+
+
+def _incidence_set(m):
+    """m directions on a cone (polar 0.3-0.8 rad) with real transverse
+    polarisations: an orientation sweep of one target."""
+    out = []
+    for q in range(m):
+        th = 0.3 + 0.5 * q / max(m - 1, 1)
+        ph = 2 * math.pi * q / m
+        d = np.array([math.sin(th) * math.cos(ph), math.sin(th) * math.sin(ph), math.cos(th)])
+        e = np.cross(d, [0.0, 0.0, 1.0])
+        out.append((d, e / np.linalg.norm(e)))
+    return out
+
+
+def _bench_directions(args, bk, stream, torch, lb, configs):
+    """Many right-hand sides of one operator: --nrhs incidence directions of
+    the Au cuboid (default 30x20x10 nm, N = 6,000, FCD, 520 nm), FP32+refine
+    to --tol.  (a) the device-assembled FP32 matrix, every FP32 step one
+    tensor-core product over all directions (lum_batch_create_rhs);
+    (b) the on-the-fly operator, two directions per pair-kernel launch
+    (lum_solve_gmres_multi)."""
+    size = tuple(float(v) for v in (args.size if args.size != "60,50,10" else "30,20,10").split(","))
+    w = configs.cuboid_au(size, 1.0, 520.0)
+    n, R = w.n, args.nrhs
+    inv = lb.invert_polarisability(w.alpha)
+    dirs = _incidence_set(R)
+    rhs = np.concatenate([lb.incident_field(w.positions, w.k, lb.IncidentField(tuple(d), tuple(e)))
+                          for d, e in dirs])
+    b_dev = torch.from_numpy(rhs).to("cuda")
+    x_dev = torch.zeros_like(b_dev)
+    tol, max_iter = args.tol, max(args.max_iter, 5000)
+    t0 = time.perf_counter()
+    C = bk.assemble_and_create_session(w.positions, w.k, inv, True, 1.0, precision="fp32")
+    torch.cuda.synchronize()
+    assemble_s = time.perf_counter() - t0
+    B = C.rhs_batch(R)
+    for _ in range(args.warmup):
+        B.solve_device(b_dev.data_ptr(), x_dev.data_ptr(), tol, max_iter, 30, "fp32_refine")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    info_tc = B.solve_device(b_dev.data_ptr(), x_dev.data_ptr(), tol, max_iter, 30, "fp32_refine")
+    torch.cuda.synchronize()
+    t_tc = time.perf_counter() - t0
+    x_tc = x_dev.cpu().numpy()
+    B.close()
+    C.close()
+    O = bk.create_onthefly_session(w.positions, inv, w.k, True, 1.0)
+    O.set_stream(stream.cuda_stream)
+    for _ in range(args.warmup):
+        O.solve_multi_device(R, b_dev.data_ptr(), x_dev.data_ptr(), tol, max_iter, 30,
+                             "fp32_refine", stream.cuda_stream)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    O.solve_multi_device(R, b_dev.data_ptr(), x_dev.data_ptr(), tol, max_iter, 30, "fp32_refine",
+                         stream.cuda_stream)
+    torch.cuda.synchronize()
+    t_otf = time.perf_counter() - t0
+    x_otf = x_dev.cpu().numpy()
+    O.close()
+    err = 0.0
+    for q, (d, e) in enumerate(dirs):
+        sl = slice(3 * n * q, 3 * n * (q + 1))
+        inc = lb.IncidentField(tuple(d), tuple(e))
+        a = lb.cross_sections(w.positions, inv, x_tc[sl], w.k, inc)[0]
+        b = lb.cross_sections(w.positions, inv, x_otf[sl], w.k, inc)[0]
+        err = max(err, abs(a - b) / abs(b))
+    its = [i["iterations"] for i in info_tc]
+    return {"metric": "dipole-solves/s, many incidence directions of one cached matrix "
+                      "(tensor-core products, FP32+refine)", "value": n * R / t_tc, "unit": UNIT,
+            "higher_is_better": True, "steps": 1, "ms_per_step": t_tc * 1e3, "scaling": "weak",
+            "dtype": "tf32x3+f64", "mode": "fp32_refine",
+            "config": {"workload": f"Au cuboid {size[0]:g}x{size[1]:g}x{size[2]:g} nm, 1 nm "
+                                   f"lattice, N={n}, FCD, 520 nm, {R} incidence directions",
+                       "n_dipoles": n, "nrhs": R, "tol": tol,
+                       "matrix_gb": 8.0 * (3 * n) ** 2 / 1e9},
+            "assemble_s": assemble_s,
+            "iterations": {"min": min(its), "max": max(its)},
+            "onthefly_two_at_a_time": {"value": n * R / t_otf, "seconds": t_otf,
+                                       "speedup_of_tensor_path": t_otf / t_tc},
+            "max_cext_rel_diff_vs_onthefly": err, "e2e": None}
 
 
 def _bench_fft(args, bk, stream, torch, lb, configs):

@@ -229,6 +229,18 @@ LUM_API int lum_batch_solve(lum_batch* b, const double* rhs, double tol, int max
 LUM_API int lum_batch_solve_device(lum_batch* b, const void* rhs_dev, void* x_dev, double tol,
                                    int max_iter, int restart, int mode, lum_solve_info* info);
 LUM_API int lum_batch_set_stream(lum_batch* b, void* stream);
+/* No counterpart in the reference, which solves one incidence at a time
+ * (cda/mod.rs:238-391): a batch of nrhs right-hand sides of one session's
+ * operator (incidence directions, polarisations), solved by lum_batch_solve
+ * with vectors stored back to back (vector r at 3N*r complex).  Each
+ * operator application takes all nrhs vectors at once: for a cached session
+ * with FP32 storage, the FP32 steps are one tensor-core product
+ * (lum_session_matmul_vectors, TENSOR); otherwise the session's operator
+ * runs two vectors at a time.  The FP64 restart residuals use the session's
+ * FP64 operator (the on-the-fly FP64 product for a device-assembled FP32
+ * matrix).  The batch borrows the session (destroy the batch first) and runs
+ * on the session's stream; at most 21,845 dipoles. */
+LUM_API int lum_batch_create_rhs(lum_session* s, int nrhs, lum_batch** out);
 /* Launch configuration: systems, dipoles, near-list width, CTAs per system
  * cluster, vector elements per thread, pair work-list items and persistent
  * grid per precision. */

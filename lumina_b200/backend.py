@@ -203,6 +203,15 @@ class CudaSession:
         _raise(self._lib.lum_session_matmul_device(self._h, c_void_p(X_ptr), c_void_p(Y_ptr),
                                                    nrhs, c_void_p(stream or None)), "matmul")
 
+    def rhs_batch(self, nrhs: int) -> "CudaBatch":
+        """A batch of ``nrhs`` right-hand sides of this session's operator
+        (lum_batch_create_rhs): solve with CudaBatch.solve on vectors stored
+        back to back.  For an FP32-storage cached session every FP32 operator
+        application is one tensor-core product over all vectors."""
+        h = c_void_p()
+        _raise(self._lib.lum_batch_create_rhs(self._h, int(nrhs), byref(h)), "rhs_batch")
+        return CudaBatch(h, [self.dim // 3] * int(nrhs), self)
+
     _METHODS = {"auto": 0, "tensor": 1, "cuda_cores": 2}
 
     def matmul(self, X: np.ndarray, method="auto") -> np.ndarray:

@@ -491,6 +491,9 @@ struct lum_batch {
   int graph_m[2] = {0, 0};
   uint64_t graph_launches[2] = {0, 0};
   int use_graph = 1;
+  // Right-hand-side batch (lum_batch_create_rhs): K vectors of one session's
+  // operator, applied through that session instead of the pair work list.
+  lum_session* src = nullptr;
   ~lum_batch() {
     for (auto& gx : graph)
       if (gx) cudaGraphExecDestroy(gx);
@@ -592,6 +595,26 @@ lum_status batch_workspace(lum_batch* B, int m) {
   return LUM_OK;
 }
 
+// y = A x for the K vectors of a right-hand-side batch.  An FP32-storage
+// cached matrix at FP32 takes the tensor-core product for all K vectors in
+// one launch; otherwise the session operator runs two vectors at a time
+// (the two-vector pair kernels for an on-the-fly session).
+lum_status rhs_apply(lum_batch* B, int prec, const double2* x, double2* y) {
+  lum_session* s = B->src;
+  const size_t n3 = (size_t)s->dim;
+  if (s->kind == 1 && s->cached.precision == LUM_FP32 && prec == LUM_FP32)
+    return s->cached.apply_multi(x, y, B->K, 1, (long long)n3, LUM_MATMUL_TENSOR, s->stream);
+  if (s->kind == 1 && s->cached.precision == LUM_FP64)
+    return s->cached.apply_multi(x, y, B->K, 1, (long long)n3, LUM_MATMUL_CUDA_CORES,
+                                 s->stream);
+  int r = 0;
+  for (; r + 1 < B->K; r += 2)
+    LUM_TRY(s->apply2(prec, x + r * n3, x + (r + 1) * n3, y + r * n3, y + (r + 1) * n3,
+                      nullptr, nullptr));
+  if (r < B->K) LUM_TRY(s->apply(prec, x + r * n3, y + r * n3));
+  return LUM_OK;
+}
+
 // One restart cycle for all systems (the body that is captured as a graph).
 lum_status batch_cycle(lum_batch* B, int mode) {
   const int prec = (mode == LUM_SOLVE_FP32_REFINE) ? LUM_FP32 : LUM_FP64;
@@ -600,13 +623,19 @@ lum_status batch_cycle(lum_batch* B, int mode) {
   const BatchFlags* fl = B->flags.as<BatchFlags>();
   LUM_TRY(dispatch_ept<RunStart>(B->ept, B));
   for (int j = 0; j < B->m; ++j) {
-    LUM_TRY(batch_apply(B->g, prec, B->V.as<double2>() + (size_t)j * len, B->w.as<double2>(),
-                        B->part.p, qa, fl, 1, B->stream));
+    if (B->src)
+      LUM_TRY(rhs_apply(B, prec, B->V.as<double2>() + (size_t)j * len, B->w.as<double2>()));
+    else
+      LUM_TRY(batch_apply(B->g, prec, B->V.as<double2>() + (size_t)j * len,
+                          B->w.as<double2>(), B->part.p, qa, fl, 1, B->stream));
     LUM_TRY(dispatch_ept<RunArnoldi>(B->ept, B, j));
   }
   LUM_TRY(dispatch_ept<RunUpdate>(B->ept, B));
-  LUM_TRY(batch_apply(B->g, LUM_FP64, B->xs.as<double2>(), B->tmp.as<double2>(), B->part.p,
-                      B->q64, fl, 2, B->stream));
+  if (B->src)
+    LUM_TRY(rhs_apply(B, LUM_FP64, B->xs.as<double2>(), B->tmp.as<double2>()));
+  else
+    LUM_TRY(batch_apply(B->g, LUM_FP64, B->xs.as<double2>(), B->tmp.as<double2>(), B->part.p,
+                        B->q64, fl, 2, B->stream));
   LUM_TRY(dispatch_ept<RunResidual>(B->ept, B));
   LUM_TRY_CUDA(cudaMemcpyAsync(B->h_active, &B->ctl.as<BatchCtl>()->active, sizeof(int),
                                cudaMemcpyDeviceToHost, B->stream));
@@ -825,6 +854,61 @@ int lum_batch_create(lum_ctx* ctx, int n_systems, const int* sys_dipoles, const 
   return LUM_OK;
 }
 
+int lum_batch_create_rhs(lum_session* s, int nrhs, lum_batch** out) {
+  if (bad_arg(s, "session") || bad_arg(out, "out")) return LUM_ERR_INVALID;
+  *out = nullptr;
+  if (nrhs <= 0) {
+    set_error("a right-hand-side batch needs at least one vector");
+    return LUM_ERR_INVALID;
+  }
+  const int n = s->n_dipoles;
+  if ((long long)n * nrhs > 50000000LL) {
+    set_error("batch too large");
+    return LUM_ERR_INVALID;
+  }
+  int ept = 0, clz = 0;
+  for (int e : {4, 8, 16, 32}) {
+    const int c = (3 * n + kBT * e - 1) / (kBT * e);
+    if (c <= kMaxCluster) {
+      ept = e;
+      clz = c;
+      break;
+    }
+  }
+  if (!ept) {
+    set_error("system of %d dipoles exceeds the batched solver's limit of %d per system", n,
+              kMaxCluster * kBT * 32 / 3);
+    return LUM_ERR_INVALID;
+  }
+  lum_batch* B = new (std::nothrow) lum_batch();
+  if (!B) return LUM_ERR_OOM;
+  B->ctx = s->ctx;
+  B->K = nrhs;
+  B->N = n * nrhs;
+  B->ept = ept;
+  B->cl = clz;
+  B->src = s;
+  B->stream = s->stream;  // the session's operator runs on its own stream
+  B->own_stream = false;
+  B->use_graph = 0;       // the operator may size its workspaces on first use
+  B->off.resize(nrhs + 1);
+  for (int r = 0; r <= nrhs; ++r) B->off[r] = r * n;
+  cudaSetDevice(s->ctx->device);
+  lum_status st = B->d_off.alloc(sizeof(int) * B->off.size());
+  if (st == LUM_OK) {
+    cudaError_t e = cudaMemcpyAsync(B->d_off.p, B->off.data(), sizeof(int) * B->off.size(),
+                                    cudaMemcpyHostToDevice, B->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(B->stream);
+    if (e != cudaSuccess) st = cuda_status(e, "rhs batch setup", __FILE__, __LINE__);
+  }
+  if (st != LUM_OK) {
+    lum_batch_destroy(B);
+    return st;
+  }
+  *out = B;
+  return LUM_OK;
+}
+
 int lum_batch_destroy(lum_batch* B) {
   if (!B) return LUM_OK;
   if (B->ctx) cudaSetDevice(B->ctx->device);
@@ -838,6 +922,11 @@ int lum_batch_destroy(lum_batch* B) {
 
 int lum_batch_set_stream(lum_batch* B, void* stream) {
   if (bad_arg(B, "batch")) return LUM_ERR_INVALID;
+  if (B->src) {  // a right-hand-side batch follows its session's stream
+    LUM_TRY((lum_status)lum_session_set_stream(B->src, stream));
+    B->stream = B->src->stream;
+    return LUM_OK;
+  }
   cudaSetDevice(B->ctx->device);
   cudaStreamSynchronize(B->stream);
   if (stream) {
@@ -875,6 +964,9 @@ int lum_batch_matvec_device(lum_batch* B, int precision, const void* x_dev, void
     return LUM_ERR_INVALID;
   }
   cudaSetDevice(B->ctx->device);
+  if (B->src)
+    return rhs_apply(B, precision, static_cast<const double2*>(x_dev),
+                     static_cast<double2*>(y_dev));
   return batch_apply(B->g, precision, static_cast<const double2*>(x_dev),
                      static_cast<double2*>(y_dev), B->part.p,
                      precision == LUM_FP32 ? B->q32 : B->q64, nullptr, 0, B->stream);
