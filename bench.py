@@ -367,13 +367,15 @@ def main():
     avg64 = ms64 / real64
     achieved = pairs * FLOPS_PER_PAIR / (avg32 * 1e-3) / 1e12
     peak = fp32_peak / 1e3
-    roof = {"bound": "fp32", "kernel": "otf_pairs_f32", "achieved": achieved, "peak": peak,
+    kcfg = sess.kernel_config()
+    kname = "otf_pairs_f32_sym" if kcfg.get("f32_sym") else "otf_pairs_f32"
+    roof = {"bound": "fp32", "kernel": kname, "achieved": achieved, "peak": peak,
             "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
             "peak_source": "FP32 FMA-chain microbenchmark in this run (MEASURED_PEAKS.json has "
                            "HBM and bf16 only); of measured",
-            "traffic": _traffic_from_profiles(), "launches": k32, "applications": real32,
+            "traffic": _traffic_from_profiles(kname), "launches": k32, "applications": real32,
             "avg_launch_ms": avg32, "flops_per_launch": pairs * FLOPS_PER_PAIR,
-            "kernel_config": sess.kernel_config(),
+            "kernel_config": kcfg,
             "fp64_kernel": {"launches": k64, "applications": real64, "avg_launch_ms": avg64,
                             "achieved_tflops": pairs * FLOPS_PER_PAIR / (avg64 * 1e-3) / 1e12,
                             "peak_tflops": fp64_peak / 1e3}}
@@ -403,8 +405,8 @@ def main():
     return 0
 
 
-def _traffic_from_profiles():
-    path = os.path.join(ROOT, "profiles", "otf_pairs_f32_cuboid30k.md")
+def _traffic_from_profiles(kernel="otf_pairs_f32"):
+    path = os.path.join(ROOT, "profiles", f"{kernel}_cuboid30k.md")
     try:
         with open(path) as f:
             for line in f:

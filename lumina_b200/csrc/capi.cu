@@ -709,11 +709,13 @@ int lum_session_kernel_config(lum_session* s, char* buf, size_t len) {
   const lum::OtfOperator& o = s->otf;
   snprintf(buf, len,
            "kind=%s f32_variant=%s tuned_ms=%.4f nsplit32=%d nsplit64=%d ell_w=%d lofree=%d "
-           "fast_trig=%d f32x2_variant=%s tuned_x2_ms=%.4f nsplit_x2=%d",
+           "fast_trig=%d f32x2_variant=%s tuned_x2_ms=%.4f nsplit_x2=%d f32_sym=%d "
+           "tuned_sym_ms=%.4f sym_superblocks=%d",
            s->kind == 0 ? "onthefly" : (s->kind == 1 ? "cached" : "fft"),
            lum::f32_variant_name(o.f32_variant),
            (double)o.tuned_ms, o.nsplit32, o.nsplit64, o.ell_w, o.lofree, o.fast_trig,
-           lum::f32x2_variant_name(o.f32x2_variant), (double)o.tuned_x2_ms, o.nsplit_x2);
+           lum::f32x2_variant_name(o.f32x2_variant), (double)o.tuned_x2_ms, o.nsplit_x2,
+           o.f32_sym, (double)o.tuned_sym_ms, o.sym_nb);
   return LUM_OK;
 }
 

@@ -119,6 +119,15 @@ struct OtfOperator {
   int f32_variant = 0;      // FP32 pair-kernel variant chosen by the tuner
   int nsplit_v[8] = {1, 1, 1, 1, 1, 1, 1, 1};
   float tuned_ms = 0.f;     // tuned FP32 pair-kernel time (ms), 0 if untuned
+  // Symmetric scheme (pairs_f32_sym.cuh): each unordered pair evaluated once
+  // over superblock pairs; chosen by the tuner when it is faster.
+  int f32_sym = 0;          // 0: split kernel; 2 or 3: symmetric kernel, CTAs per SM
+  int sym_nb = 0, sym_nitems = 0;
+  float tuned_sym_ms = 0.f;
+  DevBuf sym_items;         // int2 [sym_nitems] superblock pairs (I <= J)
+  DevBuf sym_slots;         // float2 [sym_nb][3n] per-superblock partial sums
+  lum_status sym_prepare(cudaStream_t st);
+  void sym_launch(int minb, const double2* x, const int* skip, cudaStream_t st);
   lum_status tune_f32(cudaStream_t st);
   std::vector<double> host_pos;  // double4 host copy (image positions are built from it)
 

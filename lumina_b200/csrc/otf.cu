@@ -40,6 +40,7 @@ namespace lum {
 constexpr int kOtfBlock = 128;
 }  // namespace lum
 #include "pairs_f32x2.cuh"
+#include "pairs_f32_sym.cuh"
 namespace lum {
 
 // ---------------------------------------------------------------------------
@@ -941,23 +942,84 @@ std::mutex g_tune_mu;
 std::map<std::tuple<int, int, int>, int> g_tune_cache;
 }  // namespace
 
+// Superblock pairs (I <= J) and the per-superblock partial sums of the
+// symmetric scheme (sized once per geometry).
+lum_status OtfOperator::sym_prepare(cudaStream_t st) {
+  const int nb = (n + kSymRows - 1) / kSymRows;
+  if (nb == sym_nb && sym_items.p) return LUM_OK;
+  std::vector<int2> items;
+  items.reserve((size_t)nb * (nb + 1) / 2);
+  for (int I = 0; I < nb; ++I)
+    for (int J = I; J < nb; ++J) items.push_back(make_int2(I, J));
+  LUM_TRY(sym_items.alloc(sizeof(int2) * items.size()));
+  LUM_TRY_CUDA(cudaMemcpyAsync(sym_items.p, items.data(), sizeof(int2) * items.size(),
+                               cudaMemcpyHostToDevice, st));
+  LUM_TRY(sym_slots.alloc(sizeof(float2) * (size_t)nb * 3 * (size_t)n));
+  LUM_TRY_CUDA(cudaStreamSynchronize(st));  // items is freed on return
+  sym_nb = nb;
+  sym_nitems = (int)items.size();
+  return LUM_OK;
+}
+
+template <int MINB>
+static void sym_launch_t(const OtfOperator& o, const double2* x, const int* skip,
+                         cudaStream_t st) {
+  const float kf = (float)o.k, s0f = (float)(o.k * o.k * o.k / (4.0 * kPi));
+#define LUM_SYM_LAUNCH(F, L)                                                                  \
+  otf_pairs_f32_sym<F, L, MINB><<<o.sym_nitems, kSymThreads, 0, st>>>(                        \
+      o.n, o.pos_hi.as<float4>(), o.pos_lo.as<float4>(), x, kf, s0f, o.sym_items.as<int2>(), \
+      o.sym_slots.as<float2>(), skip)
+  if (o.fast_trig && o.lofree)
+    LUM_SYM_LAUNCH(true, true);
+  else if (o.fast_trig)
+    LUM_SYM_LAUNCH(true, false);
+  else if (o.lofree)
+    LUM_SYM_LAUNCH(false, true);
+  else
+    LUM_SYM_LAUNCH(false, false);
+#undef LUM_SYM_LAUNCH
+}
+
+void OtfOperator::sym_launch(int minb, const double2* x, const int* skip, cudaStream_t st) {
+  if (minb >= 3)
+    sym_launch_t<3>(*this, x, skip, st);
+  else
+    sym_launch_t<2>(*this, x, skip, st);
+}
+
 lum_status OtfOperator::tune_f32(cudaStream_t st) {
   f32_variant = 0;
+  f32_sym = 0;
+  // LUMINA_F32_SYM=2 or 3 forces the symmetric scheme with 2 or 3 CTAs per SM
+  // (isolated systems; 1 means 2), =0
+  // excludes it; unset, the tuner decides by timing.
+  const char* sym_env = std::getenv("LUMINA_F32_SYM");
+  if (sym_env && (sym_env[0] == '2' || sym_env[0] == '3' || sym_env[0] == '1') &&
+      !has_lattice && !has_substrate) {
+    nsplit32 = nsplit_v[0];
+    f32_sym = sym_env[0] == '3' ? 3 : 2;
+    return sym_prepare(st);
+  }
+  const bool sym_allowed = !(sym_env && sym_env[0] == '0');
   const char* env = std::getenv("LUMINA_TUNE");
   if ((env && env[0] == '0') || n < 2048) {
     nsplit32 = nsplit_v[0];
     return LUM_OK;
   }
-  const auto key = std::make_tuple(n, fast_trig, lofree);
+  const auto key = std::make_tuple(n, fast_trig, lofree + 2 * (has_lattice || has_substrate) +
+                                                     4 * (sym_allowed ? 0 : 1));
+  bool known = false;
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune_cache.find(key);
     if (it != g_tune_cache.end()) {
-      f32_variant = it->second;
+      f32_variant = it->second % 100;
+      f32_sym = (!has_lattice && !has_substrate) ? it->second / 100 : 0;
       nsplit32 = nsplit_v[f32_variant];
-      return LUM_OK;
+      known = true;
     }
   }
+  if (known) return f32_sym ? sym_prepare(st) : LUM_OK;
   DevBuf xz;
   LUM_TRY(xz.alloc(sizeof(double2) * 3 * (size_t)n));
   LUM_TRY_CUDA(cudaMemsetAsync(xz.p, 0, xz.bytes, st));
@@ -995,12 +1057,40 @@ lum_status OtfOperator::tune_f32(cudaStream_t st) {
       f32_variant = v;
     }
   }
+  // the symmetric scheme (isolated systems: no lattice, no substrate image)
+  f32_sym = 0;
+  if (!has_lattice && !has_substrate && sym_allowed) {
+    LUM_TRY(sym_prepare(st));
+    tuned_sym_ms = 1e30f;
+    for (int minb = 2; minb <= 3; ++minb) {
+      float ms = 0.f;
+      for (int rep = 0; rep < 2; ++rep) {
+        cudaEventRecord(e0, st);
+        sym_launch(minb, xz.as<double2>(), nullptr, st);
+        cudaEventRecord(e1, st);
+      }
+      cudaError_t e = cudaEventSynchronize(e1);
+      if (e == cudaSuccess) e = cudaGetLastError();
+      if (e != cudaSuccess) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        return cuda_status(e, "symmetric pair-kernel tuning", __FILE__, __LINE__);
+      }
+      g_launches.fetch_add(2, std::memory_order_relaxed);
+      cudaEventElapsedTime(&ms, e0, e1);
+      tuned_sym_ms = std::min(tuned_sym_ms, ms);
+      if (ms < best) {
+        best = ms;
+        f32_sym = minb;
+      }
+    }
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   nsplit32 = nsplit_v[f32_variant];
   tuned_ms = best;
   std::lock_guard<std::mutex> lk(g_tune_mu);
-  g_tune_cache[key] = f32_variant;
+  g_tune_cache[key] = f32_variant + 100 * f32_sym;  // f32_sym: 0, 2 or 3
   return LUM_OK;
 }
 
@@ -1044,6 +1134,17 @@ lum_status OtfOperator::apply(int precision, const double2* x, double2* y, cudaS
     return LUM_OK;
   }
   const double2 rr = make_double2(substrate.refl_re, substrate.refl_im);
+  if (precision == LUM_FP32 && f32_sym) {
+    if (ev0) cudaEventRecord(ev0, st);
+    sym_launch(f32_sym, x, skip, st);
+    LUM_CHECK_LAUNCH();
+    if (ev1) cudaEventRecord(ev1, st);
+    otf_epilogue<float2, float2><<<epi_blocks, 256, 0, st>>>(
+        n, x, inv_alpha.as<double2>(), sym_slots.as<float2>(), sym_nb, ell_w, near_j.as<int>(),
+        fcd32.as<float2>(), y, skip);
+    LUM_CHECK_LAUNCH();
+    return LUM_OK;
+  }
   if (precision == LUM_FP32) {
     const F32VariantEntry& V = kF32Variants[f32_variant];
     const int ns = nsplit32;
