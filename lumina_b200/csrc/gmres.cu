@@ -14,7 +14,10 @@
 // finish sums the partials in block order, so results are deterministic.
 #include "lumina_internal.cuh"
 
+#include <cooperative_groups.h>
+
 #include <chrono>
+#include <cstdlib>
 #include <cmath>
 #include <cstddef>
 
@@ -284,6 +287,157 @@ k_mgs_final(int len, int j, MgsArgs a0, MgsArgs a1) {
   if (t <= j + 1) S->H[t * kM + j] = sH[t];
 }
 
+// The whole Arnoldi step j in one cooperative launch: the j+1 projections of
+// modified Gram-Schmidt in the order of iterative.rs:92-96, ||w||, the
+// Givens update of k_mgs_final and v_{j+1} = w / h_{j+1,j}.  Each reduction
+// crosses one grid barrier: every block writes its partial, and after the
+// barrier every block sums all partials in the same fixed order, so every
+// block holds the same h_{i,j} (deterministic, no atomics).  Partials are
+// double-buffered by barrier parity: a buffer is rewritten two barriers after
+// it was filled, when every block has read it.  All blocks pass the same
+// j + 2 barriers; a right-hand side whose cycle is done does no work but
+// still takes part, and the launch returns at once (before any barrier) only
+// when every right-hand side is done.
+__device__ double2 coop_total(const double2* part, int G) {
+  double2 v = make_double2(0.0, 0.0);
+  for (int b = threadIdx.x; b < G; b += blockDim.x) {
+    const double2 p = __ldcg(&part[b]);
+    v.x += p.x;
+    v.y += p.y;
+  }
+  v = block_sum2(v);
+  __shared__ double2 s_tot;
+  if (threadIdx.x == 0) s_tot = v;
+  __syncthreads();
+  const double2 t = s_tot;
+  __syncthreads();
+  return t;
+}
+
+__global__ void __launch_bounds__(kVecThreads)
+k_arnoldi_coop(int len, int j, int nrhs, MgsArgs a0, MgsArgs a1, double2* part0,
+               double2* part1) {
+  namespace cg = cooperative_groups;
+  cg::grid_group grid = cg::this_grid();
+  const int r = blockIdx.y;
+  const MgsArgs a = r ? a1 : a0;
+  double2* part = r ? part1 : part0;
+  const int G = gridDim.x;
+  const bool done0 = a0.S->done != 0, done1 = (nrhs > 1) ? (a1.S->done != 0) : true;
+  if (done0 && done1) return;  // grid-uniform: no barrier is taken
+  const bool active = !(r ? done1 : done0);
+  double2* __restrict__ w = a.w;
+  const double2* __restrict__ V = a.V;
+  GmresState* S = a.S;
+  const int stride = G * blockDim.x;
+  double2 hprev = make_double2(0.0, 0.0);
+  double hn = 0.0;
+  for (int i = 0; i <= j + 1; ++i) {
+    double2 acc = make_double2(0.0, 0.0);
+    if (active) {
+      const double2* vp = V + (size_t)(i > 0 ? i - 1 : 0) * len;
+      if (i <= j) {  // w -= h_{i-1,j} v_{i-1};  <v_i, w>
+        const double2* vi = V + (size_t)i * len;
+        for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < len; q += stride) {
+          double2 wq = w[q];
+          if (i > 0) {
+            const double2 t = dmul(vp[q], hprev);
+            wq.x -= t.x;
+            wq.y -= t.y;
+            w[q] = wq;
+          }
+          const double2 d = dconjmul(vi[q], wq);
+          acc.x += d.x;
+          acc.y += d.y;
+        }
+      } else {  // w -= h_{j,j} v_j;  ||w||^2
+        for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < len; q += stride) {
+          const double2 t = dmul(vp[q], hprev);
+          double2 wq = w[q];
+          wq.x -= t.x;
+          wq.y -= t.y;
+          w[q] = wq;
+          acc.x += wq.x * wq.x + wq.y * wq.y;
+        }
+      }
+    }
+    acc = block_sum2(acc);
+    double2* buf = part + (size_t)(i & 1) * G;
+    if (threadIdx.x == 0) buf[blockIdx.x] = acc;
+    grid.sync();
+    const double2 tot = coop_total(buf, G);
+    if (i <= j) {
+      hprev = tot;
+      if (active && blockIdx.x == 0 && threadIdx.x == 0) S->H[i * kM + j] = tot;
+    } else {
+      hn = sqrt(tot.x);
+    }
+  }
+  if (!active) return;
+  // v_{j+1} = w / h_{j+1,j} (iterative.rs:101-106); this block's own entries
+  {
+    double2* __restrict__ vnext = a.V + (size_t)(j + 1) * len;
+    const bool ok = hn > 1e-30;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < len; q += stride) {
+      const double2 wq = w[q];
+      vnext[q] = ok ? make_double2(wq.x / hn, wq.y / hn) : make_double2(0.0, 0.0);
+    }
+  }
+  if (blockIdx.x != 0) return;
+  // Givens update of column j (iterative.rs:98-133) on block 0, as k_mgs_final
+  __shared__ double2 sH[kM + 1], sSn[kM], sG[2];
+  __shared__ double sC[kM];
+  const int t = threadIdx.x;
+  __syncthreads();  // S->H[i][j] written by thread 0 above
+  if (t <= j) sH[t] = S->H[t * kM + j];
+  if (t < j) {
+    sC[t] = S->cs[t];
+    sSn[t] = S->sn[t];
+  }
+  if (t < 2) sG[t] = S->g[j + t];
+  __syncthreads();
+  if (t == 0) {
+    sH[j + 1] = make_double2(hn, 0.0);
+    for (int i = 0; i < j; ++i) {
+      const double c = sC[i];
+      const double2 s = sSn[i];
+      const double2 hij = sH[i], hi1 = sH[i + 1];
+      const double2 t1 = dmul(s, hi1);
+      const double2 temp = make_double2(c * hij.x + t1.x, c * hij.y + t1.y);
+      const double2 t2 = dmul(make_double2(-s.x, s.y), hij);  // -conj(s) * h_ij
+      sH[i + 1] = make_double2(t2.x + c * hi1.x, t2.y + c * hi1.y);
+      sH[i] = temp;
+    }
+    double c;
+    double2 s;
+    givens(sH[j], sH[j + 1], &c, &s);
+    const double2 hjj = sH[j], hj1 = sH[j + 1];
+    const double2 t1 = dmul(s, hj1);
+    sH[j] = make_double2(c * hjj.x + t1.x, c * hjj.y + t1.y);
+    sH[j + 1] = make_double2(0.0, 0.0);
+    const double2 gj = sG[0], gj1 = sG[1];
+    const double2 t3 = dmul(s, gj1);
+    const double2 t4 = dmul(make_double2(-s.x, s.y), gj);
+    const double2 g1 = make_double2(t4.x + c * gj1.x, t4.y + c * gj1.y);
+    S->g[j] = make_double2(c * gj.x + t3.x, c * gj.y + t3.y);
+    S->g[j + 1] = g1;
+    S->cs[j] = c;
+    S->sn[j] = s;
+    S->scal[1] = hn;
+    const double gabs = dabs(g1);
+    S->scal[2] = gabs;
+    S->jdone = j + 1;
+    if (!isfinite(gabs)) {
+      S->bad = 1;
+      S->done = 1;
+    } else if (gabs < a.abs_tol || gabs < a.inner_thr || j + 1 >= a.jmax) {
+      S->done = 1;
+    }
+  }
+  __syncthreads();
+  if (t <= j + 1) S->H[t * kM + j] = sH[t];
+}
+
 // v_{j+1} = w / h_{j+1,j}, or 0 on a lucky breakdown (iterative.rs:101-106)
 __global__ void __launch_bounds__(kVecThreads)
 k_next_basis(int len, int j, MgsArgs a0, MgsArgs a1) {
@@ -371,6 +525,7 @@ lum_status GmresWork::ensure(int len_, int m_, cudaStream_t st) {
   LUM_TRY(r.alloc(sizeof(double2) * (size_t)len));
   LUM_TRY(tmp.alloc(sizeof(double2) * (size_t)len));
   LUM_TRY(partials.alloc(sizeof(double2) * (size_t)nblk));
+  LUM_TRY(coop_part.alloc(sizeof(double2) * 2 * (size_t)nblk));
   LUM_TRY(counter.alloc(sizeof(unsigned)));
   LUM_TRY(state.alloc(sizeof(GmresState)));
   LUM_TRY_CUDA(cudaMemsetAsync(counter.p, 0, sizeof(unsigned), st));
@@ -461,6 +616,21 @@ lum_status lum_gmres_device_multi(lum_session* s, int nrhs, const double2* const
                                  cudaMemcpyDeviceToDevice, st));
     R.active = true;
   }
+  // Blocks per right-hand side of the fused step kernel: the step kernels'
+  // grid, bounded so that both right-hand sides' blocks are co-resident (a
+  // cooperative launch needs that); 0 selects the per-projection kernels
+  // (LUMINA_COOP=0, or no cooperative launch on the device).
+  int coop_blocks = 0;
+  {
+    int dev = 0, coop = 0, sms = 148, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_arnoldi_coop, kVecThreads, 0);
+    const char* env = std::getenv("LUMINA_COOP");
+    if (coop && per_sm > 0 && !(env && env[0] == '0'))
+      coop_blocks = std::max(1, std::min(run[0].W->nblk, (per_sm * sms) / nrhs));
+  }
   for (;;) {
     // the reference's loop head (iterative.rs:60-90): converged / out of steps
     int act[2], na = 0;
@@ -514,15 +684,28 @@ lum_status lum_gmres_device_multi(lum_session* s, int nrhs, const double2* const
                         (mode == LUM_SOLVE_FP32_REFINE) ? inner_rel * R.beta : 0.0, R.jmax};
       }
       if (na == 1) ma[1] = ma[0];
-      const dim3 grid(run[act[0]].W->nblk, na);
-      for (int i = 0; i <= j; ++i) {
-        k_mgs<<<grid, kVecThreads, 0, st>>>(len, i, j, ma[0], ma[1]);
+      if (coop_blocks > 0) {
+        // the whole step in one cooperative launch
+        int nr = na;
+        double2* p0 = run[act[0]].W->coop_part.as<double2>();
+        double2* p1 = run[act[na - 1]].W->coop_part.as<double2>();
+        int lenv = len, jv = j;
+        void* args[] = {&lenv, &jv, &nr, &ma[0], &ma[1], &p0, &p1};
+        LUM_TRY_CUDA(cudaLaunchCooperativeKernel((const void*)k_arnoldi_coop,
+                                                 dim3(coop_blocks, na), dim3(kVecThreads),
+                                                 args, 0, st));
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+      } else {
+        const dim3 grid(run[act[0]].W->nblk, na);
+        for (int i = 0; i <= j; ++i) {
+          k_mgs<<<grid, kVecThreads, 0, st>>>(len, i, j, ma[0], ma[1]);
+          LUM_CHECK_LAUNCH();
+        }
+        k_mgs_final<<<grid, kVecThreads, 0, st>>>(len, j, ma[0], ma[1]);
+        LUM_CHECK_LAUNCH();
+        k_next_basis<<<grid, kVecThreads, 0, st>>>(len, j, ma[0], ma[1]);
         LUM_CHECK_LAUNCH();
       }
-      k_mgs_final<<<grid, kVecThreads, 0, st>>>(len, j, ma[0], ma[1]);
-      LUM_CHECK_LAUNCH();
-      k_next_basis<<<grid, kVecThreads, 0, st>>>(len, j, ma[0], ma[1]);
-      LUM_CHECK_LAUNCH();
     }
     for (int q = 0; q < na; ++q) {
       RhsRun& R = run[act[q]];

@@ -263,6 +263,7 @@ struct GmresWork {
   int len = 0;      // complex entries (3N)
   int m = 0;
   DevBuf V, w, r, tmp, partials, counter, state;
+  DevBuf coop_part;                // double2 [2][nblk]: block sums of the fused step kernel
   GmresState* h_state = nullptr;   // pinned mirror of a few scalars
   int nblk = 0;
   lum_status ensure(int len, int m, cudaStream_t st);
