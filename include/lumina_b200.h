@@ -314,6 +314,18 @@ LUM_API int lum_far_field(lum_ctx* ctx, int n_dipoles, const double* pos, const 
                           double k, int n_theta, int n_phi, double* theta, double* phi,
                           double* intensity);
 
+/* ---- nonlinear sources (nonlinear.rs) -------------------------------------- */
+/* compute_shg_sources / compute_thg_sources (crates/lumina-core/src/
+ * nonlinear.rs:61-86, :233-258): order 2: p_a = sum chi_abc E_b E_c
+ * (Chi2Tensor, 27 complex, index a*9+b*3+c); order 3: p_a = sum chi_abcd
+ * E_b E_c E_d (Chi3Tensor, 81 complex).  local_fields and sources are 3N
+ * complex; chi holds n_tensors tensors back to back (1: one tensor for every
+ * dipole, or N).  FP64 on the device.  The harmonic response solves
+ * A(k_h) p = sources with a session at the harmonic wave number
+ * (nonlinear.rs:108-240). */
+LUM_API int lum_harmonic_sources(lum_ctx* ctx, int order, int n_dipoles, const double* local_fields,
+                                 int n_tensors, const double* chi, double* sources);
+
 /* ---- measurement --------------------------------------------------------- */
 /* While enabled, every launch of the session's dominant matvec kernel (the
  * dense pair kernel, or the GEMV of a cached session) is bracketed by CUDA

@@ -107,6 +107,7 @@ SIGNATURES = {
                                    _dp]),
     "lum_far_field": (c_int, [c_void_p, c_int, _dp, _dp, c_double, c_int, c_int, _dp, _dp,
                               _dp]),
+    "lum_harmonic_sources": (c_int, [c_void_p, c_int, c_int, _dp, c_int, _dp, _dp]),
     "lum_matvec_onthefly_noalloc": (c_int, [c_int, c_void_p, c_void_p, c_double, c_void_p,
                                             c_void_p, c_void_p]),
     "lum_batch_create": (c_int, [c_void_p, c_int, POINTER(c_int), _dp, _dp, _dp, _dp, c_int,

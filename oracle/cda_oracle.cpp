@@ -1352,6 +1352,37 @@ void orc_far_field(int n, const double* pos, const double* moments, double k, in
   }
 }
 
+// compute_shg_sources / compute_thg_sources, nonlinear.rs:61-86, :233-258,
+// with Chi2Tensor::contract / Chi3Tensor::contract (types.rs:355-365,
+// :461-472): p[a] += chi[...] * e[b] * e[c] (* e[d]) in the loop order a, b,
+// c (, d).  per_dipole = 0 uses one tensor for every dipole.
+void orc_harmonic_sources(int order, int n, const double* e_loc, int per_dipole,
+                          const double* chi, double* out) {
+  const int nc = order == 2 ? 27 : 81;
+  for (int i = 0; i < n; ++i) {
+    const double* t = chi + 2 * (size_t)nc * (per_dipole ? i : 0);
+    C e[3];
+    for (int c = 0; c < 3; ++c) e[c] = C{e_loc[2 * (3 * (size_t)i + c)], e_loc[2 * (3 * (size_t)i + c) + 1]};
+    for (int a = 0; a < 3; ++a) {
+      C p = cc(0.0);
+      for (int b = 0; b < 3; ++b)
+        for (int c = 0; c < 3; ++c) {
+          if (order == 2) {
+            const int q = a * 9 + b * 3 + c;
+            p = add(p, mul(mul(C{t[2 * q], t[2 * q + 1]}, e[b]), e[c]));
+          } else {
+            for (int d = 0; d < 3; ++d) {
+              const int q = a * 27 + b * 9 + c * 3 + d;
+              p = add(p, mul(mul(mul(C{t[2 * q], t[2 * q + 1]}, e[b]), e[c]), e[d]));
+            }
+          }
+        }
+      out[2 * (3 * (size_t)i + a)] = p.re;
+      out[2 * (3 * (size_t)i + a) + 1] = p.im;
+    }
+  }
+}
+
 // The reference's WGSL shaders, restated in FP32 (the "reference GPU
 // equivalent" of the cached path).  matrix_assemble.wgsl:21-103 and
 // matvec.wgsl:19-39; the host diagonal patch is gpu.rs:585-603.

@@ -59,6 +59,7 @@ def _load():
                                        _dp, _dp]),
         "orc_near_field_plane": (None, [_dp, _dp, c_double, c_double, c_int, c_int, _dp, _dp]),
         "orc_far_field": (None, [c_int, _dp, _dp, c_double, c_int, c_int, _dp, _dp, _dp]),
+        "orc_harmonic_sources": (None, [c_int, c_int, _dp, c_int, _dp, _dp]),
         "orc_ewald_evaluate": (None, [ctypes.c_void_p, _dp, _dp, c_double, c_int, _dp]),
         "orc_lattice_eta": (c_double, [ctypes.c_void_p]),
         "orc_erfc": (c_double, [c_double]),
@@ -383,6 +384,19 @@ def far_field(pos, moments, k, n_theta, n_phi):
     lib().orc_far_field(pos.shape[0], _p(pos), _p(mom.view(np.float64)), k, n_theta, n_phi,
                         _p(th), _p(ph), _p(it))
     return th, ph, it
+
+
+def harmonic_sources(order, local_fields, chi):
+    """compute_shg_sources / compute_thg_sources (nonlinear.rs): (N, 3) complex.
+    chi: one tensor (27 or 81 complex) or N of them."""
+    e = np.ascontiguousarray(np.asarray(local_fields, np.complex128).reshape(-1))
+    n = e.size // 3
+    nc = 27 if order == 2 else 81
+    t = np.ascontiguousarray(np.asarray(chi, np.complex128).reshape(-1, nc))
+    out = np.zeros(3 * n, np.complex128)
+    lib().orc_harmonic_sources(order, n, _p(e.view(np.float64)), int(t.shape[0] > 1),
+                               _p(t.view(np.float64)), _p(out.view(np.float64)))
+    return out.reshape(-1, 3)
 
 
 def circular_dichroism(mom_x, mom_y, k):
