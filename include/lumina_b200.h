@@ -79,6 +79,18 @@ typedef struct {
   double refl_im;
 } lum_substrate;
 
+/* SubstrateRuntime::Sommerfeld (solver/substrate.rs:109-113, built by
+ * from_spec at :126-130 as SommerfeldGreens::new(wavelength_nm, eps_sub,
+ * eps_env), sommerfeld.rs:236-241): the full reflected Green's tensor by the
+ * Sommerfeld integral over k_par. */
+typedef struct {
+  double z_interface;
+  double wavelength_nm;
+  double eps_sub_re;
+  double eps_sub_im;
+  double eps_env;
+} lum_sommerfeld;
+
 typedef struct {
   int iterations;          /* Arnoldi steps, counted as iterative.rs:129 does */
   int restarts;            /* restart cycles completed */
@@ -161,6 +173,37 @@ LUM_API int lum_session_create_fft(lum_ctx* ctx, int n_dipoles, const double* po
  * per-wavelength loop, runner.rs:150-183). */
 LUM_API int lum_session_set_wavelength(lum_session* s, double k, const double* inv_alpha,
                                const lum_substrate* substrate);
+/* The Sommerfeld substrate runtime in the sessions.  Replaces the
+ * SubstrateRuntime::Sommerfeld arms of assemble_interaction_matrix
+ * (assembly.rs:157-166) and matvec_on_the_fly (assembly.rs:296-303): every
+ * block (i, j), i == j included, gets -G_refl(r_i, r_j).  The integrals of
+ * each unordered pair are evaluated once on the device into a table of
+ * 32 N(N+1) bytes (N <= 65535), which the on-the-fly application streams and
+ * the dense assembly folds into the matrix.  Arguments as
+ * lum_session_assemble / lum_session_create_onthefly with `somm` in place of
+ * the Fresnel substrate. */
+LUM_API int lum_session_assemble_sommerfeld(lum_ctx* ctx, int n_dipoles, const double* pos,
+                                            const double* inv_alpha, double k, int use_fcd,
+                                            double cell_size, const lum_lattice* lattice,
+                                            const double k_bloch[3], const lum_sommerfeld* somm,
+                                            int storage_precision, lum_session** out);
+LUM_API int lum_session_create_onthefly_sommerfeld(lum_ctx* ctx, int n_dipoles,
+                                                   const double* pos, const double* inv_alpha,
+                                                   double k, int use_fcd, double cell_size,
+                                                   const lum_lattice* lattice,
+                                                   const double k_bloch[3],
+                                                   const lum_sommerfeld* somm,
+                                                   lum_session** out);
+/* Rebuilds the Sommerfeld table of an on-the-fly session for new substrate
+ * parameters (after lum_session_set_wavelength, which marks the table stale:
+ * until it is rebuilt the session's applications fail with INVALID), or
+ * re-assembles a cached session's matrix with them. */
+LUM_API int lum_session_set_sommerfeld(lum_session* s, const lum_sommerfeld* somm);
+/* SommerfeldGreens::evaluate (sommerfeld.rs:254-300) on the device for
+ * npairs point pairs: ri, rj are npairs x 3, g receives npairs x 3 x 3
+ * interleaved complex values. */
+LUM_API int lum_sommerfeld_tensor(lum_ctx* ctx, const lum_sommerfeld* somm, int npairs,
+                                  const double* ri, const double* rj, double* g);
 /* MatvecSession::matvec (backend.rs:54, gpu.rs:428-488) on host vectors,
  * precision LUM_FP64 or LUM_FP32 (FP32 arithmetic, FP64 in/out). */
 LUM_API int lum_session_matvec(lum_session* s, int precision, const double* x, double* y);

@@ -10,7 +10,7 @@ from .backend import (ComputeError, ConvergenceFailure, CudaBackend, CudaBatch, 
                       DeviceError,
                       InvalidGeometry, OutOfMemory, SolverError, Unavailable, cross_sections,
                       incident_field, invert_polarisability)
-from .lattice import LatticeSpec, SubstrateRuntime, SubstrateSpec
+from .lattice import LatticeSpec, SommerfeldRuntime, SubstrateRuntime, SubstrateSpec
 from .solver import CdaSolver, circular_dichroism
 from .types import (CrossSections, Dipole, DipoleResponse, DipoleSet, IncidentField,
                     SimulationParams, clausius_mossotti, ellipsoid_polarisability_tensor,
@@ -19,7 +19,7 @@ from .types import (CrossSections, Dipole, DipoleResponse, DipoleSet, IncidentFi
 __all__ = [
     "CudaBackend", "CudaSession", "CudaBatch", "CdaSolver", "ComputeError", "Unavailable", "DeviceError",
     "OutOfMemory", "SolverError", "ConvergenceFailure", "InvalidGeometry", "LatticeSpec",
-    "SubstrateSpec", "SubstrateRuntime", "Dipole", "DipoleSet", "IncidentField",
+    "SubstrateSpec", "SubstrateRuntime", "SommerfeldRuntime", "Dipole", "DipoleSet", "IncidentField",
     "SimulationParams", "CrossSections", "DipoleResponse", "clausius_mossotti",
     "radiative_correction", "ellipsoid_polarisability_tensor", "wavenumber",
     "invert_polarisability", "incident_field", "cross_sections", "circular_dichroism",

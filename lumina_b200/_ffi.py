@@ -46,6 +46,11 @@ class LumSubstrate(ctypes.Structure):
     _fields_ = [("z_interface", c_double), ("refl_re", c_double), ("refl_im", c_double)]
 
 
+class LumSommerfeld(ctypes.Structure):
+    _fields_ = [("z_interface", c_double), ("wavelength_nm", c_double), ("eps_sub_re", c_double),
+                ("eps_sub_im", c_double), ("eps_env", c_double)]
+
+
 class LumSolveInfo(ctypes.Structure):
     _fields_ = [
         ("iterations", c_int),
@@ -80,6 +85,14 @@ SIGNATURES = {
                                             c_double, c_void_p, _dp, c_void_p,
                                             POINTER(c_void_p)]),
     "lum_session_set_wavelength": (c_int, [c_void_p, c_double, _dp, c_void_p]),
+    "lum_session_assemble_sommerfeld": (c_int, [c_void_p, c_int, _dp, _dp, c_double, c_int,
+                                                c_double, c_void_p, _dp, c_void_p, c_int,
+                                                POINTER(c_void_p)]),
+    "lum_session_create_onthefly_sommerfeld": (c_int, [c_void_p, c_int, _dp, _dp, c_double,
+                                                       c_int, c_double, c_void_p, _dp, c_void_p,
+                                                       POINTER(c_void_p)]),
+    "lum_session_set_sommerfeld": (c_int, [c_void_p, c_void_p]),
+    "lum_sommerfeld_tensor": (c_int, [c_void_p, c_void_p, c_int, _dp, _dp, _dp]),
     "lum_session_create_fft": (c_int, [c_void_p, c_int, _dp, _dp, c_double, c_int, c_double,
                                        c_double, POINTER(c_void_p)]),
     "lum_session_matvec": (c_int, [c_void_p, c_int, _dp, _dp]),

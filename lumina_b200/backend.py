@@ -18,7 +18,7 @@ from typing import Optional
 import numpy as np
 
 from . import _ffi
-from ._ffi import LumLattice, LumSolveInfo, LumSubstrate
+from ._ffi import LumLattice, LumSolveInfo, LumSommerfeld, LumSubstrate
 
 
 class ComputeError(Exception):
@@ -110,6 +110,16 @@ def lattice_struct(lattice) -> Optional[LumLattice]:
     s.truncation_real = int(lattice.truncation_real)
     s.truncation_recip = int(lattice.truncation_recip)
     return s
+
+
+def _is_sommerfeld(substrate) -> bool:
+    return substrate is not None and hasattr(substrate, "wavelength_nm")
+
+
+def sommerfeld_struct(somm) -> LumSommerfeld:
+    e = complex(somm.eps_sub)
+    return LumSommerfeld(float(somm.z_interface), float(somm.wavelength_nm), e.real, e.imag,
+                         float(somm.eps_env))
 
 
 def substrate_struct(substrate) -> Optional[LumSubstrate]:
@@ -240,10 +250,21 @@ class CudaSession:
         _raise(self._lib.lum_session_set_stream(self._h, c_void_p(stream or None)), "set_stream")
 
     def set_wavelength(self, k: float, inv_alpha: np.ndarray, substrate=None) -> None:
+        """Re-targets the session (runner.rs:150-183); a SommerfeldRuntime
+        substrate rebuilds the session's reflected-tensor table."""
         ia = _c128(inv_alpha, 9 * (self.dim // 3))
-        sub = substrate_struct(substrate)
+        somm = _is_sommerfeld(substrate)
+        sub = None if somm else substrate_struct(substrate)
         _raise(self._lib.lum_session_set_wavelength(self._h, float(k), _dp(ia.view(np.float64)),
                                                     _ref(sub)), "set_wavelength")
+        if somm:
+            self.set_sommerfeld(substrate)
+
+    def set_sommerfeld(self, somm) -> None:
+        """Rebuilds the Sommerfeld reflected-tensor table (and an assembled
+        matrix) for ``somm`` (a SommerfeldRuntime)."""
+        st = sommerfeld_struct(somm)
+        _raise(self._lib.lum_session_set_sommerfeld(self._h, byref(st)), "set_sommerfeld")
 
     # -- solve --------------------------------------------------------------
     def solve(self, rhs: np.ndarray, tol: float = 1e-6, max_iter: int = 1000, restart: int = 30,
@@ -532,8 +553,15 @@ class CudaBackend:
         n = pos.shape[0]
         ia = _c128(diagonal_blocks, 9 * n)
         kb = np.asarray(k_bloch, np.float64)
-        lat, sub = lattice_struct(lattice), substrate_struct(substrate)
         h = c_void_p()
+        if _is_sommerfeld(substrate):
+            st = sommerfeld_struct(substrate)
+            _raise(self._lib.lum_session_assemble_sommerfeld(
+                self._h, n, _dp(pos), _dp(ia.view(np.float64)), float(k), int(bool(use_fcd)),
+                float(cell_size), _ref(lattice_struct(lattice)), _dp(kb), byref(st),
+                _prec(precision), byref(h)), "assemble")
+            return CudaSession(h, 3 * n, "cached", self)
+        lat, sub = lattice_struct(lattice), substrate_struct(substrate)
         _raise(self._lib.lum_session_assemble(self._h, n, _dp(pos), _dp(ia.view(np.float64)),
                                               float(k), int(bool(use_fcd)), float(cell_size),
                                               _ref(lat), _dp(kb), _ref(sub), _prec(precision),
@@ -561,8 +589,15 @@ class CudaBackend:
         n = pos.shape[0]
         ia = _c128(inv_alpha, 9 * n)
         kb = np.asarray(k_bloch, np.float64)
-        lat, sub = lattice_struct(lattice), substrate_struct(substrate)
         h = c_void_p()
+        if _is_sommerfeld(substrate):
+            st = sommerfeld_struct(substrate)
+            _raise(self._lib.lum_session_create_onthefly_sommerfeld(
+                self._h, n, _dp(pos), _dp(ia.view(np.float64)), float(k), int(bool(use_fcd)),
+                float(cell_size), _ref(lattice_struct(lattice)), _dp(kb), byref(st), byref(h)),
+                "create_onthefly")
+            return CudaSession(h, 3 * n, "onthefly", self)
+        lat, sub = lattice_struct(lattice), substrate_struct(substrate)
         _raise(self._lib.lum_session_create_onthefly(self._h, n, _dp(pos),
                                                      _dp(ia.view(np.float64)), float(k),
                                                      int(bool(use_fcd)), float(cell_size),
@@ -594,6 +629,19 @@ class CudaBackend:
                                           _dp(IA.view(np.float64)), _dp(K), _dp(C),
                                           int(bool(use_fcd)), byref(h)), "create_batch")
         return CudaBatch(h, sizes, self)
+
+    def sommerfeld_tensor(self, somm, ri, rj) -> np.ndarray:
+        """SommerfeldGreens::evaluate (sommerfeld.rs:254-300) on the device for
+        point pairs (ri, rj: (P, 3) or (3,)); returns (P, 3, 3) or (3, 3)."""
+        a = np.ascontiguousarray(np.asarray(ri, np.float64).reshape(-1, 3))
+        b = np.ascontiguousarray(np.asarray(rj, np.float64).reshape(-1, 3))
+        if a.shape != b.shape:
+            raise InvalidGeometry(f"pair arrays differ: {a.shape} vs {b.shape}")
+        g = np.zeros((a.shape[0], 3, 3), np.complex128)
+        st = sommerfeld_struct(somm)
+        _raise(self._lib.lum_sommerfeld_tensor(self._h, byref(st), a.shape[0], _dp(a), _dp(b),
+                                               _dp(g.view(np.float64))), "sommerfeld_tensor")
+        return g if np.ndim(ri) > 1 else g[0]
 
     def dense_solve(self, matrix, rhs):
         """The reference's default (backend.rs:123-133): no dense LU here;

@@ -288,7 +288,10 @@ lum_status CachedOperator::assemble(const OtfOperator& g, cudaStream_t st) {
     set_error("matrix too large for device assembly");
     return LUM_ERR_INVALID;
   }
-  if (g.has_lattice && g.table_ok) return assemble_from_table(g, precision, A.p, ld, st);
+  if (g.has_lattice && g.table_ok) {
+    LUM_TRY(assemble_from_table(g, precision, A.p, ld, st));
+    return somm_assemble(g, precision, A.p, ld, st);
+  }
   if (precision == LUM_FP32)
     assemble_pairs<float2><<<(unsigned)blocks, threads, 0, st>>>(
         n, g.pos64.as<double4>(), g.inv_alpha.as<double2>(), g.k, g.has_lattice, g.latdev,
@@ -310,7 +313,7 @@ lum_status CachedOperator::assemble(const OtfOperator& g, cudaStream_t st) {
           n, g.ell_w, g.near_j.as<int>(), g.fcd64.as<double2>(), ld, A.as<double2>());
     LUM_CHECK_LAUNCH();
   }
-  return LUM_OK;
+  return somm_assemble(g, precision, A.p, ld, st);
 }
 
 lum_status CachedOperator::apply(const double2* x, double2* y, cudaStream_t st,

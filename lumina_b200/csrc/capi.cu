@@ -91,11 +91,17 @@ lum_status lum_session::apply(int precision, const double2* x, double2* y, const
     e0 = r.a;
     e1 = r.b;
   }
-  if (kind == 0) return otf.apply(precision, x, y, stream, e0, e1, skip);
+  if (kind == 0) {
+    LUM_TRY(otf.apply(precision, x, y, stream, e0, e1, skip));
+    return otf.somm_apply(x, y, stream, skip);
+  }
   if (kind == 2) return fft.apply(precision, x, y, stream, e0, e1, skip);
   // cached session
-  if (precision == LUM_FP64 && cached.precision == LUM_FP32 && otf.inv_alpha.p)
-    return otf.apply(LUM_FP64, x, y, stream, nullptr, nullptr, skip);
+  if (otf.has_somm && otf.somm_stale) return otf.somm_apply(x, y, stream, skip);  // error
+  if (precision == LUM_FP64 && cached.precision == LUM_FP32 && otf.inv_alpha.p) {
+    LUM_TRY(otf.apply(LUM_FP64, x, y, stream, nullptr, nullptr, skip));
+    return otf.somm_apply(x, y, stream, skip);
+  }
   if (e0) cudaEventRecord(e0, stream);
   LUM_TRY(cached.apply(x, y, stream, skip));
   if (e1) cudaEventRecord(e1, stream);
@@ -125,7 +131,9 @@ lum_status lum_session::apply2(int precision, const double2* x, const double2* x
     e0 = r.a;
     e1 = r.b;
   }
-  return otf.apply2(precision, x, x2, y, y2, stream, e0, e1, skip, skip2);
+  LUM_TRY(otf.apply2(precision, x, x2, y, y2, stream, e0, e1, skip, skip2));
+  LUM_TRY(otf.somm_apply(x, y, stream, skip));
+  return otf.somm_apply(x2, y2, stream, skip2);
 }
 
 static bool bad_ptr(const void* p, const char* what) {
@@ -427,10 +435,17 @@ int lum_session_set_wavelength(lum_session* s, double k, const double* inv_alpha
     return LUM_ERR_INVALID;
   }
   LUM_TRY(check_physics(s->n_dipoles, inv_alpha, k));
+  if (s->otf.has_somm && substrate) {
+    set_error("a Sommerfeld session takes no Fresnel substrate");
+    return LUM_ERR_INVALID;
+  }
   cudaSetDevice(s->ctx->device);
   LUM_TRY(s->otf.set_physics(k, inv_alpha, s->otf.use_fcd, s->otf.cell, nullptr, nullptr,
                              substrate, s->stream));
-  if (s->kind == 1) LUM_TRY(s->cached.assemble(s->otf, s->stream));
+  // The Sommerfeld table (and a matrix built from it) waits for
+  // lum_session_set_sommerfeld with this wavelength's substrate.
+  if (s->otf.has_somm) s->otf.somm_stale = 1;
+  else if (s->kind == 1) LUM_TRY(s->cached.assemble(s->otf, s->stream));
   LUM_TRY_CUDA(cudaStreamSynchronize(s->stream));
   return LUM_OK;
 }
@@ -480,6 +495,81 @@ int lum_session_assemble(lum_ctx* ctx, int n, const double* pos, const double* i
     return st;
   }
   *out = s;
+  return LUM_OK;
+}
+
+// Sessions with the Sommerfeld substrate runtime (assembly.rs:157-166 and
+// :296-303): the free-space or lattice operator plus -G_refl from the
+// device table (sommerfeld.cu).
+int lum_session_create_onthefly_sommerfeld(lum_ctx* ctx, int n, const double* pos,
+                                           const double* inv_alpha, double k, int use_fcd,
+                                           double cell, const lum_lattice* lattice,
+                                           const double k_bloch[3], const lum_sommerfeld* somm,
+                                           lum_session** out) {
+  if (bad_ptr(ctx, "ctx") || bad_ptr(out, "out") || bad_ptr(somm, "somm")) return LUM_ERR_INVALID;
+  *out = nullptr;
+  lum_session* s = nullptr;
+  LUM_TRY((lum_status)lum_session_create_onthefly(ctx, n, pos, inv_alpha, k, use_fcd, cell,
+                                                  lattice, k_bloch, nullptr, &s));
+  lum_status st = s->otf.somm_build(somm, s->stream);
+  if (st == LUM_OK) {
+    cudaError_t e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) st = cuda_status(e, "Sommerfeld table", __FILE__, __LINE__);
+  }
+  if (st != LUM_OK) {
+    lum_session_destroy(s);
+    return st;
+  }
+  *out = s;
+  return LUM_OK;
+}
+
+int lum_session_assemble_sommerfeld(lum_ctx* ctx, int n, const double* pos,
+                                    const double* inv_alpha, double k, int use_fcd, double cell,
+                                    const lum_lattice* lattice, const double k_bloch[3],
+                                    const lum_sommerfeld* somm, int precision,
+                                    lum_session** out) {
+  if (bad_ptr(ctx, "ctx") || bad_ptr(out, "out") || bad_ptr(somm, "somm")) return LUM_ERR_INVALID;
+  *out = nullptr;
+  LUM_TRY(check_inputs(n, pos, inv_alpha, k));
+  if (precision != LUM_FP32 && precision != LUM_FP64) {
+    set_error("invalid storage precision %d", precision);
+    return LUM_ERR_INVALID;
+  }
+  lum_session* s = nullptr;
+  LUM_TRY(new_session(ctx, 1, 3 * n, &s));
+  lum_status st = s->otf.build_geometry(pos, n, s->stream);
+  if (st == LUM_OK)
+    st = s->otf.set_physics(k, inv_alpha, use_fcd, cell, lattice, k_bloch, nullptr, s->stream);
+  if (st == LUM_OK) st = s->otf.somm_build(somm, s->stream);
+  if (st == LUM_OK) st = s->cached.allocate(3 * n, precision);
+  if (st == LUM_OK) st = s->cached.assemble(s->otf, s->stream);
+  if (st == LUM_OK) {
+    cudaError_t e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) st = cuda_status(e, "assembly", __FILE__, __LINE__);
+  }
+  if (st != LUM_OK) {
+    lum_session_destroy(s);
+    return st;
+  }
+  *out = s;
+  return LUM_OK;
+}
+
+int lum_session_set_sommerfeld(lum_session* s, const lum_sommerfeld* somm) {
+  if (bad_ptr(s, "session") || bad_ptr(somm, "somm")) return LUM_ERR_INVALID;
+  if (s->kind == 2 || !s->otf.inv_alpha.p) {
+    set_error("the Sommerfeld substrate needs an on-the-fly or assembled session");
+    return LUM_ERR_INVALID;
+  }
+  if (s->otf.has_substrate) {
+    set_error("the session already has a Fresnel substrate");
+    return LUM_ERR_INVALID;
+  }
+  cudaSetDevice(s->ctx->device);
+  LUM_TRY(s->otf.somm_build(somm, s->stream));
+  if (s->kind == 1) LUM_TRY(s->cached.assemble(s->otf, s->stream));
+  LUM_TRY_CUDA(cudaStreamSynchronize(s->stream));
   return LUM_OK;
 }
 

@@ -86,6 +86,15 @@ struct SubstrateDev {
   double refl_re, refl_im;
 };
 
+// SommerfeldGreens (sommerfeld.rs:215-241) with the interface height.
+struct SommDev {
+  double z0;
+  double k_env;
+  double eps_env;
+  double2 eps_sub;
+  double2 k_sub;
+};
+
 // --- on-the-fly operator ----------------------------------------------------
 struct OtfOperator {
   int n = 0;                // dipoles
@@ -130,6 +139,16 @@ struct OtfOperator {
   void sym_launch(int minb, const double2* x, const int* skip, cudaStream_t st);
   lum_status tune_f32(cudaStream_t st);
   std::vector<double> host_pos;  // double4 host copy (image positions are built from it)
+
+  // Sommerfeld substrate (sommerfeld.cu): the reflected-tensor integrals of
+  // every unordered pair, evaluated once per wavelength into an HBM table of
+  // 64-byte records; each application streams the table (y -= G_refl x).
+  int has_somm = 0;
+  int somm_stale = 0;        // the physics changed after the table was built
+  SommDev somm{};
+  DevBuf somm_tab;           // double2 [n(n+1)/2][4]
+  lum_status somm_build(const lum_sommerfeld* s, cudaStream_t st);
+  lum_status somm_apply(const double2* x, double2* y, cudaStream_t st, const int* skip) const;
 
   // Periodic (Ewald) operator on a dipole lattice: every displacement is
   // d*(da, db, dc) with integer steps, so the periodic tensor is tabulated
@@ -329,6 +348,8 @@ int batch_occupancy(const BatchGeom& g, int precision);                         
 
 const char* f32_variant_name(int v);    // otf.cu
 const char* f32x2_variant_name(int v);  // otf.cu
+lum_status somm_assemble(const OtfOperator& g, int precision, void* A, size_t ld,
+                         cudaStream_t st);
 lum_status assemble_from_table(const OtfOperator& g, int precision, void* A, size_t ld,
                                cudaStream_t st);  // table.cu
 

@@ -1,0 +1,499 @@
+// sommerfeld.cu -- the substrate's reflected Green's tensor by the Sommerfeld
+// integral (crates/lumina-core/src/solver/sommerfeld.rs) on the device, FP64.
+//
+// G_refl(r_i, r_j) depends on the pair only through the lateral distance
+// rho, the height sum dz = (z_i - z0) + (z_j - z0) and the azimuth phi.  The
+// expensive part -- five k_par integrals by 15-node Kronrod quadrature on up
+// to three segments (45 integrand evaluations, each with two complex square
+// roots, two complex divisions, a complex exponential and J0/J1) -- is a
+// function of (rho, dz) alone, which is symmetric in i and j.  So, once per
+// wavelength, one thread per unordered pair evaluates the integrals and keeps
+// four pre-multiplied complex values (64 B) in an HBM table:
+//
+//   A = pre (I_s_J0 + I_p_J0),  B = pre I_J2,  Z = pre I_zz,  X = pre I_xz,
+//   pre = i / (8 pi)                                    (sommerfeld.rs:281)
+//
+// and every use rebuilds the 3x3 block from the ordered pair's own (dx, dy):
+//
+//   G_xx = A - B cos2phi   G_yy = A + B cos2phi   G_zz = -Z
+//   G_xy = -B sin2phi      G_xz = X cos phi       G_yz = X sin phi
+//
+// (sommerfeld.rs:284-289; cos phi = dx / rho, sin phi = dy / rho, phi = 0 at
+// rho = 0 as atan2(0, 0) gives).  The operator application y -= G_refl x
+// (assembly.rs:296-303, every j including i) streams the table, one warp per
+// row; the dense assembly (assembly.rs:157-166) subtracts the same blocks
+// from the stored matrix.  The stand-alone evaluator follows evaluate()
+// (sommerfeld.rs:254-300) literally for parity checks.
+#include "lumina_internal.cuh"
+#include "device_physics.cuh"
+
+#include <cmath>
+
+namespace lum {
+
+// Kronrod 15-point rule on [-1, 1] (sommerfeld.rs:43-76).
+__constant__ double c_somm_x[15] = {
+    -0.991455371120813, -0.949107912342758, -0.864864423359769, -0.741531185599394,
+    -0.586087235467691, -0.405845151377397, -0.207784955007898, 0.0,
+    0.207784955007898,  0.405845151377397,  0.586087235467691,  0.741531185599394,
+    0.864864423359769,  0.949107912342758,  0.991455371120813};
+__constant__ double c_somm_w[15] = {
+    0.022935322010529, 0.063092092629979, 0.104790010322250, 0.140653259715525,
+    0.169004726639267, 0.190350578064785, 0.204432940075298, 0.209482141084728,
+    0.204432940075298, 0.190350578064785, 0.169004726639267, 0.140653259715525,
+    0.104790010322250, 0.063092092629979, 0.022935322010529};
+
+// J0 and J1 with the coefficients of sommerfeld.rs:103-146.  Their x >= 8
+// branches (and four small-x J1 coefficients) are that module's own, not the
+// Numerical Recipes values used for the lattice sums; the reflected tensor is
+// defined by them, so they are kept as written.
+__device__ __forceinline__ double somm_j0(double x) {
+  const double ax = fabs(x);
+  if (ax < 8.0) {
+    const double y = x * x;
+    const double p1 = 57568490574.0 + y * (-13362590354.0 + y * (651619640.7 +
+                      y * (-11214424.18 + y * (77392.33017 + y * (-184.9052456)))));
+    const double q1 = 57568490411.0 + y * (1029532985.0 + y * (9494680.718 +
+                      y * (59272.64853 + y * (267.8532712 + y))));
+    return p1 / q1;
+  }
+  const double z = 8.0 / ax, y = z * z, xx = ax - 0.7853981634;
+  const double p1 = 1.0 + y * (-0.001098628627 + y * (0.000002734511 +
+                    y * (-0.00000002073 + y * (-0.0000000002073))));
+  const double q1 = -0.001562499995 + y * (0.000001430488 + y * (-0.000000006905 +
+                    y * (0.0000000001077 + y * 0.00000000000272)));
+  double s, c;
+  sincos(xx, &s, &c);
+  return sqrt(2.0 / (kPi * ax)) * (p1 * c - z * q1 * s);
+}
+
+__device__ __forceinline__ double somm_j1(double x) {
+  const double ax = fabs(x);
+  double val;
+  if (ax < 8.0) {
+    const double y = x * x;
+    const double p1 = x * (72362614232.0 + y * (-7895059235.0 + y * (242396853.1 +
+                      y * (-2972611.439 + y * (15704.4882 + y * (-30.1635081))))));
+    const double q1 = 144725228442.0 + y * (2300535178.0 + y * (18583304.74 +
+                      y * (99447.43526 + y * (376.9949199 + y))));
+    val = p1 / q1;
+  } else {
+    const double z = 8.0 / ax, y = z * z, xx = ax - 2.356194491;
+    const double p1 = 1.0 + y * (0.000183105 + y * (-0.0000035163965 +
+                      y * (0.00000002457572 + y * 2.457520e-7)));
+    const double q1 = 0.040957605 + y * (-0.000004976877 + y * (0.0000000798216 +
+                      y * (-0.000000000944603 + y * 4.53491e-10)));
+    double s, c;
+    sincos(xx, &s, &c);
+    val = sqrt(2.0 / (kPi * ax)) * (p1 * c - z * q1 * s);
+  }
+  return x < 0.0 ? -val : val;
+}
+
+// Principal square root with Im >= 0 (csqrt_pos_im, sommerfeld.rs:161-164).
+// Algebraic form of the principal branch; agrees with the polar form to
+// rounding.
+__device__ __forceinline__ double2 somm_csqrt(double2 z) {
+  double2 s;
+  if (z.y == 0.0) {
+    if (!signbit(z.x)) {
+      s = make_double2(sqrt(z.x), z.y);
+    } else {
+      const double im = sqrt(-z.x);
+      s = make_double2(0.0, signbit(z.y) ? -im : im);
+    }
+  } else {
+    const double r = hypot(z.x, z.y);
+    const double t = sqrt(0.5 * (r + fabs(z.x)));
+    if (z.x >= 0.0)
+      s = make_double2(t, z.y / (2.0 * t));
+    else
+      s = make_double2(fabs(z.y) / (2.0 * t), copysign(t, z.y));
+  }
+  if (s.y < 0.0) s = make_double2(-s.x, -s.y);
+  return s;
+}
+
+__device__ __forceinline__ double2 cscale(double2 a, double s) {
+  return make_double2(a.x * s, a.y * s);
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) {
+  return make_double2(a.x + b.x, a.y + b.y);
+}
+
+struct SommInt {
+  double2 s_j0, p_j0, zz, xz, j2;
+};
+
+// The five integrands at one k_par (sommerfeld.rs:376-413).  k_z in the
+// environment is either real (propagating) or imaginary (evanescent), so
+// k_z^2 = k^2 - k_par^2 is real and the phase is a pure rotation or a pure
+// decay.
+__device__ __forceinline__ void somm_integrand(const SommDev& S, double kpar, double rho,
+                                               double dz, double w, SommInt& acc) {
+  const double k = S.k_env, k2 = k * k;
+  const double q = k2 - kpar * kpar;          // k_z^2 (real)
+  double2 kz, factor, phase;                  // k_z, k_par / k_z, exp(i k_z dz)
+  if (q >= 0.0) {
+    const double r = sqrt(q);
+    kz = make_double2(r, 0.0);
+    factor = make_double2(kpar / r, 0.0);
+    double s, c;
+    sincos(r * dz, &s, &c);
+    phase = make_double2(c, s);
+  } else {
+    const double r = sqrt(-q);
+    kz = make_double2(0.0, r);
+    factor = make_double2(0.0, -kpar / r);
+    phase = make_double2(exp(-r * dz), 0.0);
+  }
+  const double a = k2 / S.eps_env;
+  const double2 kzs = somm_csqrt(make_double2(S.eps_sub.x * a - kpar * kpar, S.eps_sub.y * a));
+  const double2 r_s = cdiv(make_double2(kz.x - kzs.x, kz.y - kzs.y),
+                           make_double2(kz.x + kzs.x, kz.y + kzs.y));
+  const double2 ek = cmul(S.eps_sub, kz);
+  const double2 r_p = cdiv(make_double2(ek.x - S.eps_env * kzs.x, ek.y - S.eps_env * kzs.y),
+                           make_double2(ek.x + S.eps_env * kzs.x, ek.y + S.eps_env * kzs.y));
+  const double arg = kpar * rho;
+  const double j0v = somm_j0(arg), j1v = somm_j1(arg);
+  const double j2v = fabs(arg) < 1e-15 ? 0.0 : (2.0 / arg) * j1v - j0v;
+  const double2 F = cmul(phase, factor);
+  const double2 rsF = cmul(r_s, F), rpF = cmul(r_p, F);
+  const double qk = q / k2, pk = kpar * kpar / k2;
+  acc.s_j0 = cadd(acc.s_j0, cscale(rsF, w * j0v));
+  acc.p_j0 = cadd(acc.p_j0, cscale(rpF, w * qk * j0v));
+  acc.zz = cadd(acc.zz, cscale(rpF, w * pk * j0v));
+  acc.j2 = cadd(acc.j2, cscale(rpF, w * qk * j2v));
+  const double2 kzp = cmul(kz, phase);
+  acc.xz = cadd(acc.xz, cscale(cmul(r_p, kzp), w * (kpar / k) * (1.0 / k) * j1v));
+}
+
+__device__ __forceinline__ void somm_segment(const SommDev& S, double lo, double hi, double rho,
+                                             double dz, SommInt& tot) {
+  const double mid = 0.5 * (lo + hi), half = 0.5 * (hi - lo);
+  SommInt acc;
+  acc.s_j0 = acc.p_j0 = acc.zz = acc.xz = acc.j2 = make_double2(0.0, 0.0);
+#pragma unroll 1
+  for (int q = 0; q < 15; ++q)
+    somm_integrand(S, mid + half * c_somm_x[q], rho, dz, c_somm_w[q] * half, acc);
+  tot.s_j0 = cadd(tot.s_j0, acc.s_j0);
+  tot.p_j0 = cadd(tot.p_j0, acc.p_j0);
+  tot.zz = cadd(tot.zz, acc.zz);
+  tot.xz = cadd(tot.xz, acc.xz);
+  tot.j2 = cadd(tot.j2, acc.j2);
+}
+
+// integrate (sommerfeld.rs:316-352): [0, k_env], [k_env, Re k_sub] when
+// Re k_sub > 1.001 k_env, then up to k_max = max(10 ln 10 / dz, 5 k_env).
+__device__ SommInt somm_integrals(const SommDev& S, double rho, double dz) {
+  SommInt tot;
+  tot.s_j0 = tot.p_j0 = tot.zz = tot.xz = tot.j2 = make_double2(0.0, 0.0);
+  const double k_env = S.k_env;
+  const double k_sub_real = fmax(S.k_sub.x, k_env);
+  const bool seg2 = S.k_sub.x > k_env * 1.001;
+  const double k_max = dz > 1e-6 ? fmax(10.0 * 2.302585092994045684 / dz, k_env * 5.0)
+                                 : k_env * 20.0;
+  somm_segment(S, 0.0, k_env, rho, dz, tot);
+  if (seg2) somm_segment(S, k_env, k_sub_real, rho, dz, tot);
+  const double lo = seg2 ? k_sub_real : k_env;
+  if (k_max > lo * 1.001) somm_segment(S, lo, k_max, rho, dz, tot);
+  return tot;
+}
+
+// The 3x3 block from a table record and the ordered pair's (dx, dy).
+__device__ __forceinline__ void somm_block(const double2* __restrict__ rec, double dx, double dy,
+                                           double2 g[9]) {
+  const double r2 = dx * dx + dy * dy;
+  double cp = 1.0, sp = 0.0;
+  if (r2 > 0.0) {
+    const double inv = rsqrt(r2);
+    cp = dx * inv;
+    sp = dy * inv;
+  }
+  const double c2 = 2.0 * cp * cp - 1.0, s2 = 2.0 * sp * cp;
+  const double2 A = rec[0], B = rec[1], Z = rec[2], X = rec[3];
+  g[0] = make_double2(A.x - B.x * c2, A.y - B.y * c2);
+  g[4] = make_double2(A.x + B.x * c2, A.y + B.y * c2);
+  g[8] = make_double2(-Z.x, -Z.y);
+  g[1] = g[3] = make_double2(-B.x * s2, -B.y * s2);
+  g[2] = g[6] = make_double2(X.x * cp, X.y * cp);
+  g[5] = g[7] = make_double2(X.x * sp, X.y * sp);
+}
+
+// Packed upper-triangle index of the unordered pair (i <= j).
+__device__ __forceinline__ size_t somm_index(int i, int j, int n) {
+  return (size_t)i * n - ((size_t)i * (i - 1)) / 2 + (size_t)(j - i);
+}
+
+constexpr int kSommBlock = 128;
+constexpr int kSommRecord = 4;   // double2 per table record
+
+// One thread per unordered pair (i = blockIdx.y, j >= i).
+__global__ void __launch_bounds__(kSommBlock)
+somm_table(int n, const double4* __restrict__ pos, SommDev S, double2* __restrict__ tab) {
+  const int i = blockIdx.y;
+  const int j = blockIdx.x * kSommBlock + threadIdx.x;
+  if (j < i || j >= n) return;
+  const double4 ri = pos[i], rj = pos[j];
+  const double dz = (ri.z - S.z0) + (rj.z - S.z0);
+  double2* rec = tab + kSommRecord * somm_index(i, j, n);
+  if (dz <= 0.0) {
+    for (int c = 0; c < kSommRecord; ++c) rec[c] = make_double2(0.0, 0.0);
+    return;
+  }
+  const double dx = ri.x - rj.x, dy = ri.y - rj.y;
+  const SommInt I = somm_integrals(S, sqrt(dx * dx + dy * dy), dz);
+  const double pw = 1.0 / (8.0 * kPi);   // pre = i pw: (a + ib) pre = (-b pw, a pw)
+  const double2 sp = cadd(I.s_j0, I.p_j0);
+  rec[0] = make_double2(-sp.y * pw, sp.x * pw);
+  rec[1] = make_double2(-I.j2.y * pw, I.j2.x * pw);
+  rec[2] = make_double2(-I.zz.y * pw, I.zz.x * pw);
+  rec[3] = make_double2(-I.xz.y * pw, I.xz.x * pw);
+}
+
+// y_i -= sum_j G_refl(i, j) x_j: one warp per row, lanes over j, FP64,
+// fixed-order shuffle reduction (deterministic).
+constexpr int kSommRows = 8;
+__global__ void __launch_bounds__(32 * kSommRows)
+somm_apply_rows(int n, const double4* __restrict__ pos, const double2* __restrict__ tab,
+                const double2* __restrict__ x, double2* __restrict__ y,
+                const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  const int i = blockIdx.x * kSommRows + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (i >= n) return;
+  const double4 ri = pos[i];
+  const size_t base_i = somm_index(i, i, n);
+  double2 acc[3] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
+  for (int j = lane; j < n; j += 32) {
+    const size_t p = j >= i ? base_i + (size_t)(j - i) : somm_index(j, i, n);
+    const double4 rj = pos[j];
+    double2 g[9];
+    somm_block(tab + kSommRecord * p, ri.x - rj.x, ri.y - rj.y, g);
+    const double2 x0 = x[3 * (size_t)j], x1 = x[3 * (size_t)j + 1], x2 = x[3 * (size_t)j + 2];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const double2 t = cadd(cadd(cmul(g[3 * a], x0), cmul(g[3 * a + 1], x1)), cmul(g[3 * a + 2], x2));
+      acc[a] = cadd(acc[a], t);
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+    for (int o = 16; o > 0; o >>= 1) {
+      acc[a].x += __shfl_xor_sync(0xffffffffu, acc[a].x, o);
+      acc[a].y += __shfl_xor_sync(0xffffffffu, acc[a].y, o);
+    }
+  if (lane == 0)
+    for (int a = 0; a < 3; ++a) {
+      double2& e = y[3 * (size_t)i + a];
+      e = make_double2(e.x - acc[a].x, e.y - acc[a].y);
+    }
+}
+
+template <typename T2> __device__ __forceinline__ T2 somm_mk(double re, double im);
+template <> __device__ __forceinline__ float2 somm_mk<float2>(double re, double im) {
+  return make_float2((float)re, (float)im);
+}
+template <> __device__ __forceinline__ double2 somm_mk<double2>(double re, double im) {
+  return make_double2(re, im);
+}
+
+// A[i][j] -= G_refl(i, j) for every ordered pair (assembly.rs:157-166).
+template <typename T2>
+__global__ void __launch_bounds__(kSommBlock)
+somm_assemble_pairs(int n, const double4* __restrict__ pos, const double2* __restrict__ tab,
+                    size_t ld, T2* __restrict__ A) {
+  const int i = blockIdx.y;
+  const int j = blockIdx.x * kSommBlock + threadIdx.x;
+  if (j >= n) return;
+  const double4 ri = pos[i], rj = pos[j];
+  const size_t p = j >= i ? somm_index(i, j, n) : somm_index(j, i, n);
+  double2 g[9];
+  somm_block(tab + kSommRecord * p, ri.x - rj.x, ri.y - rj.y, g);
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) {
+      T2& e = A[(3 * (size_t)i + a) * ld + 3 * (size_t)j + b];
+      e = somm_mk<T2>((double)e.x - g[3 * a + b].x, (double)e.y - g[3 * a + b].y);
+    }
+}
+
+// evaluate() literally (sommerfeld.rs:254-300), one thread per pair.
+__global__ void somm_evaluate(int npairs, SommDev S, const double* __restrict__ ri,
+                              const double* __restrict__ rj, double2* __restrict__ out) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= npairs) return;
+  const double* a = ri + 3 * (size_t)q;
+  const double* b = rj + 3 * (size_t)q;
+  double2* g = out + 9 * (size_t)q;
+  const double dz = (a[2] - S.z0) + (b[2] - S.z0);
+  if (dz <= 0.0) {
+    for (int e = 0; e < 9; ++e) g[e] = make_double2(0.0, 0.0);
+    return;
+  }
+  const double dx = a[0] - b[0], dy = a[1] - b[1];
+  const double rho = sqrt(dx * dx + dy * dy);
+  const double phi = atan2(dy, dx);
+  double sp, cp;
+  sincos(phi, &sp, &cp);
+  const double c2 = 2.0 * cp * cp - 1.0, s2 = 2.0 * sp * cp;
+  const SommInt I = somm_integrals(S, rho, dz);
+  const double2 pre = make_double2(0.0, 1.0 / (8.0 * kPi));
+  const double2 spv = cadd(I.s_j0, I.p_j0);
+  g[0] = cmul(pre, make_double2(spv.x - I.j2.x * c2, spv.y - I.j2.y * c2));
+  g[4] = cmul(pre, make_double2(spv.x + I.j2.x * c2, spv.y + I.j2.y * c2));
+  g[8] = cmul(pre, make_double2(-I.zz.x, -I.zz.y));
+  g[1] = g[3] = cmul(pre, make_double2(-I.j2.x * s2, -I.j2.y * s2));
+  g[2] = g[6] = cmul(pre, cscale(I.xz, cp));
+  g[5] = g[7] = cmul(pre, cscale(I.xz, sp));
+}
+
+// SommerfeldGreens::new (sommerfeld.rs:236-241).
+lum_status somm_params(const lum_sommerfeld* s, SommDev* out) {
+  if (!s) {
+    set_error("Sommerfeld parameters must not be NULL");
+    return LUM_ERR_INVALID;
+  }
+  if (!(s->wavelength_nm > 0.0) || !std::isfinite(s->wavelength_nm) || !(s->eps_env > 0.0) ||
+      !std::isfinite(s->eps_env) || !std::isfinite(s->eps_sub_re) ||
+      !std::isfinite(s->eps_sub_im) || !std::isfinite(s->z_interface)) {
+    set_error("invalid Sommerfeld substrate (wavelength %g, eps_env %g)", s->wavelength_nm,
+              s->eps_env);
+    return LUM_ERR_INVALID;
+  }
+  const double k0 = 2.0 * kPi / s->wavelength_nm;
+  SommDev S;
+  S.z0 = s->z_interface;
+  S.k_env = k0 * std::sqrt(s->eps_env);
+  S.eps_env = s->eps_env;
+  S.eps_sub = make_double2(s->eps_sub_re, s->eps_sub_im);
+  // k_sub = csqrt_pos_im(eps_sub k0^2): principal root of a complex number
+  // (the same algebraic branch as somm_csqrt, on the host)
+  const double zr = s->eps_sub_re * k0 * k0, zi = s->eps_sub_im * k0 * k0;
+  double sr, si;
+  if (zi == 0.0) {
+    if (!std::signbit(zr)) {
+      sr = std::sqrt(zr);
+      si = zi;
+    } else {
+      sr = 0.0;
+      si = std::signbit(zi) ? -std::sqrt(-zr) : std::sqrt(-zr);
+    }
+  } else {
+    const double r = std::hypot(zr, zi);
+    const double t = std::sqrt(0.5 * (r + std::fabs(zr)));
+    if (zr >= 0.0) {
+      sr = t;
+      si = zi / (2.0 * t);
+    } else {
+      sr = std::fabs(zi) / (2.0 * t);
+      si = std::copysign(t, zi);
+    }
+  }
+  if (si < 0.0) {
+    sr = -sr;
+    si = -si;
+  }
+  S.k_sub = make_double2(sr, si);
+  *out = S;
+  return LUM_OK;
+}
+
+lum_status OtfOperator::somm_build(const lum_sommerfeld* s, cudaStream_t st) {
+  SommDev S;
+  LUM_TRY(somm_params(s, &S));
+  if (n > 65535) {
+    set_error("Sommerfeld substrate: at most 65535 dipoles (got %d)", n);
+    return LUM_ERR_INVALID;
+  }
+  const size_t pairs = (size_t)n * (n + 1) / 2;
+  const size_t bytes = pairs * kSommRecord * sizeof(double2);
+  if (somm_tab.bytes != bytes) {
+    somm_tab.release();
+    size_t free_b = 0, total_b = 0;
+    LUM_TRY_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    if (bytes + ((size_t)1 << 30) > free_b) {
+      set_error("Sommerfeld table of %zu bytes does not fit (%zu bytes free)", bytes, free_b);
+      return LUM_ERR_OOM;
+    }
+    LUM_TRY(somm_tab.alloc(bytes));
+  }
+  dim3 grid((n + kSommBlock - 1) / kSommBlock, n);
+  somm_table<<<grid, kSommBlock, 0, st>>>(n, pos64.as<double4>(), S, somm_tab.as<double2>());
+  LUM_CHECK_LAUNCH();
+  somm = S;
+  has_somm = 1;
+  somm_stale = 0;
+  return LUM_OK;
+}
+
+lum_status OtfOperator::somm_apply(const double2* x, double2* y, cudaStream_t st,
+                                   const int* skip) const {
+  if (!has_somm) return LUM_OK;
+  if (somm_stale) {
+    set_error("the Sommerfeld table belongs to another wavelength: call "
+              "lum_session_set_sommerfeld after lum_session_set_wavelength");
+    return LUM_ERR_INVALID;
+  }
+  somm_apply_rows<<<(n + kSommRows - 1) / kSommRows, 32 * kSommRows, 0, st>>>(
+      n, pos64.as<double4>(), somm_tab.as<double2>(), x, y, skip);
+  LUM_CHECK_LAUNCH();
+  return LUM_OK;
+}
+
+lum_status somm_assemble(const OtfOperator& g, int precision, void* A, size_t ld,
+                         cudaStream_t st) {
+  if (!g.has_somm) return LUM_OK;
+  dim3 grid((g.n + kSommBlock - 1) / kSommBlock, g.n);
+  if (precision == LUM_FP32)
+    somm_assemble_pairs<float2><<<grid, kSommBlock, 0, st>>>(
+        g.n, g.pos64.as<double4>(), g.somm_tab.as<double2>(), ld, (float2*)A);
+  else
+    somm_assemble_pairs<double2><<<grid, kSommBlock, 0, st>>>(
+        g.n, g.pos64.as<double4>(), g.somm_tab.as<double2>(), ld, (double2*)A);
+  LUM_CHECK_LAUNCH();
+  return LUM_OK;
+}
+
+}  // namespace lum
+
+using namespace lum;
+
+int lum_sommerfeld_tensor(lum_ctx* ctx, const lum_sommerfeld* s, int npairs, const double* ri,
+                          const double* rj, double* g) {
+  if (!ctx) {
+    set_error("null context");
+    return LUM_ERR_INVALID;
+  }
+  SommDev S;
+  LUM_TRY(somm_params(s, &S));
+  if (npairs < 0 || (npairs > 0 && (!ri || !rj || !g))) {
+    set_error("invalid pair arrays (npairs = %d)", npairs);
+    return LUM_ERR_INVALID;
+  }
+  if (npairs == 0) return LUM_OK;
+  for (size_t q = 0; q < 3 * (size_t)npairs; ++q)
+    if (!std::isfinite(ri[q]) || !std::isfinite(rj[q])) {
+      set_error("non-finite point in pair %zu", q / 3);
+      return LUM_ERR_INVALID;
+    }
+  LUM_TRY_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = nullptr;
+  LUM_TRY_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  struct StreamGuard {
+    cudaStream_t s;
+    ~StreamGuard() { cudaStreamDestroy(s); }
+  } guard{st};
+  DevBuf da, db, dg;
+  const size_t pb = sizeof(double) * 3 * (size_t)npairs;
+  LUM_TRY(da.alloc(pb));
+  LUM_TRY(db.alloc(pb));
+  LUM_TRY(dg.alloc(sizeof(double2) * 9 * (size_t)npairs));
+  LUM_TRY_CUDA(cudaMemcpyAsync(da.p, ri, pb, cudaMemcpyHostToDevice, st));
+  LUM_TRY_CUDA(cudaMemcpyAsync(db.p, rj, pb, cudaMemcpyHostToDevice, st));
+  somm_evaluate<<<(npairs + 127) / 128, 128, 0, st>>>(npairs, S, da.as<double>(),
+                                                      db.as<double>(), dg.as<double2>());
+  LUM_CHECK_LAUNCH();
+  LUM_TRY_CUDA(cudaMemcpyAsync(g, dg.p, dg.bytes, cudaMemcpyDeviceToHost, st));
+  LUM_TRY_CUDA(cudaStreamSynchronize(st));
+  return LUM_OK;
+}

@@ -68,9 +68,24 @@ def substrate_reflection_factor(eps_sub: complex, eps_env: float, use_retarded: 
 
 @dataclass
 class SubstrateSpec:
+    """SubstrateSpec (solver/substrate.rs:56-83); ``use_sommerfeld`` selects
+    the full Sommerfeld-integral reflected tensor and overrides
+    ``use_retarded``."""
     z_interface: float = 0.0
     material: str = ""
     use_retarded: bool = True
+    use_sommerfeld: bool = False
+
+
+@dataclass
+class SommerfeldRuntime:
+    """SubstrateRuntime::Sommerfeld (solver/substrate.rs:109-113): the
+    interface plane and the SommerfeldGreens parameters (sommerfeld.rs:
+    236-241), evaluated on the device by the sessions."""
+    z_interface: float
+    wavelength_nm: float
+    eps_sub: complex
+    eps_env: float
 
 
 @dataclass
@@ -80,6 +95,14 @@ class SubstrateRuntime:
     delta_eps: complex
 
     @staticmethod
-    def from_spec(spec: SubstrateSpec, eps_sub: complex, eps_env: float) -> "SubstrateRuntime":
+    def from_spec(spec: SubstrateSpec, eps_sub: complex, eps_env: float,
+                  wavelength_nm: Optional[float] = None):
+        """SubstrateRuntime::from_spec (substrate.rs:125-137): the Fresnel
+        runtime, or a SommerfeldRuntime when ``spec.use_sommerfeld``."""
+        if spec.use_sommerfeld:
+            if wavelength_nm is None:
+                raise ValueError("the Sommerfeld substrate needs the wavelength")
+            return SommerfeldRuntime(float(spec.z_interface), float(wavelength_nm),
+                                     complex(eps_sub), float(eps_env))
         return SubstrateRuntime(spec.z_interface,
                                 substrate_reflection_factor(eps_sub, eps_env, spec.use_retarded))

@@ -1597,3 +1597,260 @@ int orc_max_threads(void) {
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Sommerfeld reflected Green's tensor of a planar substrate
+// (crates/lumina-core/src/solver/sommerfeld.rs) and the Sommerfeld substrate
+// runtime (solver/substrate.rs:109-113, 126-130) in the assembly
+// (assembly.rs:157-166) and the on-the-fly matvec (assembly.rs:296-303).
+// ===========================================================================
+namespace {
+
+// Kronrod 15-point nodes and weights on [-1, 1], sommerfeld.rs:43-76.
+const double SOMM_GK_X[15] = {
+    -0.991455371120813, -0.949107912342758, -0.864864423359769, -0.741531185599394,
+    -0.586087235467691, -0.405845151377397, -0.207784955007898, 0.0,
+    0.207784955007898,  0.405845151377397,  0.586087235467691,  0.741531185599394,
+    0.864864423359769,  0.949107912342758,  0.991455371120813};
+const double SOMM_GK_W[15] = {
+    0.022935322010529, 0.063092092629979, 0.104790010322250, 0.140653259715525,
+    0.169004726639267, 0.190350578064785, 0.204432940075298, 0.209482141084728,
+    0.204432940075298, 0.190350578064785, 0.169004726639267, 0.140653259715525,
+    0.104790010322250, 0.063092092629979, 0.022935322010529};
+
+// J0 of sommerfeld.rs:103-121.  The x >= 8 coefficients are the module's
+// own (they are not the Numerical Recipes values of the Ewald module); they
+// are restated as written because the reflected tensor is built from them.
+double somm_j0(double x) {
+  double ax = std::fabs(x);
+  if (ax < 8.0) {
+    double y = x * x;
+    double p1 = 57568490574.0 + y * (-13362590354.0 + y * (651619640.7 + y * (-11214424.18 +
+                y * (77392.33017 + y * (-184.9052456)))));
+    double q1 = 57568490411.0 + y * (1029532985.0 + y * (9494680.718 + y * (59272.64853 +
+                y * (267.8532712 + y))));
+    return p1 / q1;
+  }
+  double z = 8.0 / ax, y = z * z, xx = ax - 0.7853981634;
+  double p1 = 1.0 + y * (-0.001098628627 + y * (0.000002734511 + y * (-0.00000002073 +
+              y * (-0.0000000002073))));
+  double q1 = -0.001562499995 + y * (0.000001430488 + y * (-0.000000006905 +
+              y * (0.0000000001077 + y * 0.00000000000272)));
+  return std::sqrt(2.0 / (PI * ax)) * (p1 * std::cos(xx) - z * q1 * std::sin(xx));
+}
+
+// J1 of sommerfeld.rs:126-146 (module's own coefficients, as above).
+double somm_j1(double x) {
+  double ax = std::fabs(x), val;
+  if (ax < 8.0) {
+    double y = x * x;
+    double p1 = x * (72362614232.0 + y * (-7895059235.0 + y * (242396853.1 + y * (-2972611.439 +
+                y * (15704.4882 + y * (-30.1635081))))));
+    double q1 = 144725228442.0 + y * (2300535178.0 + y * (18583304.74 + y * (99447.43526 +
+                y * (376.9949199 + y))));
+    val = p1 / q1;
+  } else {
+    double z = 8.0 / ax, y = z * z, xx = ax - 2.356194491;
+    double p1 = 1.0 + y * (0.000183105 + y * (-0.0000035163965 + y * (0.00000002457572 +
+                y * 2.457520e-7)));
+    double q1 = 0.040957605 + y * (-0.000004976877 + y * (0.0000000798216 +
+                y * (-0.000000000944603 + y * 4.53491e-10)));
+    val = std::sqrt(2.0 / (PI * ax)) * (p1 * std::cos(xx) - z * q1 * std::sin(xx));
+  }
+  return x < 0.0 ? -val : val;
+}
+
+// sommerfeld.rs:150-153
+double somm_j2(double x) {
+  if (std::fabs(x) < 1e-15) return 0.0;
+  return (2.0 / x) * somm_j1(x) - somm_j0(x);
+}
+
+struct Somm {
+  double k_env;
+  C k_sub;
+  C eps_sub;
+  double eps_env;
+};
+
+// SommerfeldGreens::new, sommerfeld.rs:236-241
+Somm somm_new(double wavelength_nm, C eps_sub, double eps_env) {
+  double k0 = 2.0 * PI / wavelength_nm;
+  Somm S;
+  S.k_env = k0 * std::sqrt(eps_env);
+  S.k_sub = csqrt_pos_imag(mul(eps_sub, cc(k0 * k0, 0.0)));
+  S.eps_sub = eps_sub;
+  S.eps_env = eps_env;
+  return S;
+}
+
+struct SommI {
+  C s_j0, p_j0, zz, xz, j2;
+};
+
+// integrand, sommerfeld.rs:376-413
+SommI somm_integrand(const Somm& S, double kpar, double rho, double dz) {
+  double k = S.k_env, k2 = k * k;
+  C kz_env = csqrt_pos_imag(cc(k2 - kpar * kpar, 0.0));
+  C kz_sub = csqrt_pos_imag(sub(mul(S.eps_sub, cc(k2 / S.eps_env, 0.0)), cc(kpar * kpar, 0.0)));
+  C r_s = div(sub(kz_env, kz_sub), add(kz_env, kz_sub));
+  C ee = cc(S.eps_env, 0.0);
+  C r_p = div(sub(mul(S.eps_sub, kz_env), mul(ee, kz_sub)),
+              add(mul(S.eps_sub, kz_env), mul(ee, kz_sub)));
+  C phase = cexp(muls(mul(cc(0.0, 1.0), kz_env), dz));
+  double arg = kpar * rho;
+  C j0v = cc(somm_j0(arg)), j1v = cc(somm_j1(arg)), j2v = cc(somm_j2(arg));
+  C kpar_c = cc(kpar), k2_c = cc(k2);
+  C kz_factor = div(kpar_c, kz_env);
+  C kz2 = div(mul(kz_env, kz_env), k2_c);
+  SommI o;
+  o.s_j0 = mul(mul(mul(r_s, j0v), phase), kz_factor);
+  o.p_j0 = mul(mul(mul(mul(r_p, kz2), j0v), phase), kz_factor);
+  o.zz = mul(mul(mul(mul(r_p, div(mul(kpar_c, kpar_c), k2_c)), j0v), phase), kz_factor);
+  o.xz = mul(mul(mul(mul(r_p, div(kpar_c, cc(k))), div(kz_env, cc(k))), j1v), phase);
+  o.j2 = mul(mul(mul(mul(r_p, kz2), j2v), phase), kz_factor);
+  return o;
+}
+
+// integrate_segment, sommerfeld.rs:355-373 (Kronrod weights x half-width)
+void somm_segment(const Somm& S, double a, double b, double rho, double dz, SommI& tot) {
+  double mid = 0.5 * (a + b), half = 0.5 * (b - a);
+  SommI acc{cc(0), cc(0), cc(0), cc(0), cc(0)};
+  for (int q = 0; q < 15; ++q) {
+    double kpar = mid + half * SOMM_GK_X[q];
+    double w = SOMM_GK_W[q] * half;
+    SommI c = somm_integrand(S, kpar, rho, dz);
+    acc.s_j0 = add(acc.s_j0, muls(c.s_j0, w));
+    acc.p_j0 = add(acc.p_j0, muls(c.p_j0, w));
+    acc.zz = add(acc.zz, muls(c.zz, w));
+    acc.xz = add(acc.xz, muls(c.xz, w));
+    acc.j2 = add(acc.j2, muls(c.j2, w));
+  }
+  tot.s_j0 = add(tot.s_j0, acc.s_j0);
+  tot.p_j0 = add(tot.p_j0, acc.p_j0);
+  tot.zz = add(tot.zz, acc.zz);
+  tot.xz = add(tot.xz, acc.xz);
+  tot.j2 = add(tot.j2, acc.j2);
+}
+
+// integrate, sommerfeld.rs:316-352: [0, k_env], [k_env, Re k_sub] when
+// Re k_sub > 1.001 k_env, and [max(k_env, Re k_sub), k_max].
+SommI somm_integrate(const Somm& S, double rho, double dz) {
+  double k_env = S.k_env;
+  double k_sub_real = std::max(S.k_sub.re, k_env);
+  bool has_seg2 = S.k_sub.re > k_env * 1.001;
+  double k_max = dz > 1e-6 ? std::max(10.0 * 2.302585092994045684 / dz, k_env * 5.0) : k_env * 20.0;
+  SommI tot{cc(0), cc(0), cc(0), cc(0), cc(0)};
+  somm_segment(S, 0.0, k_env, rho, dz, tot);
+  if (has_seg2) somm_segment(S, k_env, k_sub_real, rho, dz, tot);
+  double lo = has_seg2 ? k_sub_real : k_env;
+  if (k_max > lo * 1.001) somm_segment(S, lo, k_max, rho, dz, tot);
+  return tot;
+}
+
+// evaluate, sommerfeld.rs:254-300
+void somm_tensor(const Somm& S, const double* ri, const double* rj, double z0, T3 g) {
+  double dz = (ri[2] - z0) + (rj[2] - z0);
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) g[a][b] = cc(0.0);
+  if (dz <= 0.0) return;
+  double dx = ri[0] - rj[0], dy = ri[1] - rj[1];
+  double rho = std::sqrt(dx * dx + dy * dy);
+  double phi = std::atan2(dy, dx);
+  double cp = std::cos(phi), sp = std::sin(phi);
+  double c2 = 2.0 * cp * cp - 1.0, s2 = 2.0 * sp * cp;
+  SommI I = somm_integrate(S, rho, dz);
+  C pre = cc(0.0, 1.0 / (8.0 * PI));
+  C sp_sum = add(I.s_j0, I.p_j0);
+  g[0][0] = mul(pre, sub(sp_sum, muls(I.j2, c2)));
+  g[1][1] = mul(pre, add(sp_sum, muls(I.j2, c2)));
+  g[2][2] = mul(pre, neg(I.zz));
+  g[0][1] = g[1][0] = mul(pre, muls(neg(I.j2), s2));
+  g[0][2] = g[2][0] = mul(pre, muls(I.xz, cp));
+  g[1][2] = g[2][1] = mul(pre, muls(I.xz, sp));
+}
+
+}  // namespace
+
+extern "C" {
+
+/* SommerfeldGreens parameters (SubstrateRuntime::from_spec, substrate.rs:126-130). */
+typedef struct {
+  double z_interface;
+  double wavelength_nm;
+  double eps_sub_re, eps_sub_im;
+  double eps_env;
+} orc_sommerfeld;
+
+static Somm somm_of(const orc_sommerfeld* s) {
+  return somm_new(s->wavelength_nm, cc(s->eps_sub_re, s->eps_sub_im), s->eps_env);
+}
+
+double orc_somm_bessel(int which, double x) {
+  return which == 0 ? somm_j0(x) : which == 1 ? somm_j1(x) : somm_j2(x);
+}
+
+// G_refl for npairs (ri, rj) pairs, 9 interleaved complex values each.
+void orc_sommerfeld_tensor(const orc_sommerfeld* s, int npairs, const double* ri,
+                           const double* rj, double* out, int nthreads) {
+  Somm S = somm_of(s);
+  int nt = set_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 16) num_threads(nt)
+  for (int p = 0; p < npairs; ++p) {
+    T3 g;
+    somm_tensor(S, ri + 3 * (size_t)p, rj + 3 * (size_t)p, s->z_interface, g);
+    store_t3(g, out + 18 * (size_t)p);
+  }
+}
+
+// assemble_interaction_matrix with SubstrateRuntime::Sommerfeld
+// (assembly.rs:157-166): the free-space / lattice matrix minus G_refl for
+// every (i, j), i == j included.
+int orc_assemble_sommerfeld(int n, const double* pos, const double* alpha, double k, int use_fcd,
+                            double cell, const orc_lattice* lat, const double* kb,
+                            const orc_sommerfeld* s, double* A, int nthreads) {
+  int st = orc_assemble(n, pos, alpha, k, use_fcd, cell, lat, kb, nullptr, A, nthreads);
+  if (st) return st;
+  Somm S = somm_of(s);
+  const size_t dim = 3 * (size_t)n;
+  C* M = reinterpret_cast<C*>(A);
+  int nt = set_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nt)
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) {
+      T3 g;
+      somm_tensor(S, pos + 3 * (size_t)i, pos + 3 * (size_t)j, s->z_interface, g);
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) {
+          C& e = M[(3 * i + r) * dim + 3 * j + c];
+          e = sub(e, g[r][c]);
+        }
+    }
+  return 0;
+}
+
+// matvec_on_the_fly with SubstrateRuntime::Sommerfeld (assembly.rs:296-303).
+int orc_matvec_sommerfeld(int n, const double* pos, const double* alpha, const double* x,
+                          double k, int use_fcd, double cell, const orc_lattice* lat,
+                          const double* kb, const orc_sommerfeld* s, double* y, int nthreads) {
+  int st = orc_matvec_onthefly(n, pos, alpha, x, k, use_fcd, cell, lat, kb, nullptr, y, nthreads);
+  if (st) return st;
+  Somm S = somm_of(s);
+  const C* xv = reinterpret_cast<const C*>(x);
+  C* yv = reinterpret_cast<C*>(y);
+  int nt = set_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nt)
+  for (int i = 0; i < n; ++i) {
+    C yi[3] = {yv[3 * i], yv[3 * i + 1], yv[3 * i + 2]};
+    for (int j = 0; j < n; ++j) {
+      T3 g;
+      somm_tensor(S, pos + 3 * (size_t)i, pos + 3 * (size_t)j, s->z_interface, g);
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) yi[a] = sub(yi[a], mul(g[a][b], xv[3 * j + b]));
+    }
+    for (int a = 0; a < 3; ++a) yv[3 * i + a] = yi[a];
+  }
+  return 0;
+}
+
+}  // extern "C"

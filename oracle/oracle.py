@@ -40,6 +40,11 @@ class OrcSubstrate(ctypes.Structure):
     _fields_ = [("z_interface", c_double), ("refl_re", c_double), ("refl_im", c_double)]
 
 
+class OrcSommerfeld(ctypes.Structure):
+    _fields_ = [("z_interface", c_double), ("wavelength_nm", c_double), ("eps_sub_re", c_double),
+                ("eps_sub_im", c_double), ("eps_env", c_double)]
+
+
 def build() -> str:
     """Compile the oracle library in place (g++, OpenMP)."""
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
@@ -92,6 +97,12 @@ def _load():
         "orc_grad_cext": (c_int, [c_int, _dp, _dp, c_double, c_int, c_double, _dp, _dp,
                                   c_double, ctypes.c_void_p, _dp, _dp, _dp, _dp, c_int]),
         "orc_max_threads": (c_int, []),
+        "orc_somm_bessel": (c_double, [c_int, c_double]),
+        "orc_sommerfeld_tensor": (None, [ctypes.c_void_p, c_int, _dp, _dp, _dp, c_int]),
+        "orc_assemble_sommerfeld": (c_int, [c_int, _dp, _dp, c_double, c_int, c_double,
+                                            ctypes.c_void_p, _dp, ctypes.c_void_p, _dp, c_int]),
+        "orc_matvec_sommerfeld": (c_int, [c_int, _dp, _dp, _dp, c_double, c_int, c_double,
+                                          ctypes.c_void_p, _dp, ctypes.c_void_p, _dp, c_int]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -138,6 +149,12 @@ def _sub(substrate):
         return None
     r = complex(substrate.delta_eps)
     return OrcSubstrate(float(substrate.z_interface), r.real, r.imag)
+
+
+def _somm(somm):
+    e = complex(somm.eps_sub)
+    return OrcSommerfeld(float(somm.z_interface), float(somm.wavelength_nm), e.real, e.imag,
+                         float(somm.eps_env))
 
 
 def _ref(struct):
@@ -443,3 +460,58 @@ def grad_cext(pos, alpha, k, use_fcd=False, cell_size=3.0, direction=(0, 0, 1),
     if st:
         raise RuntimeError(f"orc_grad_cext failed ({st})")
     return c_ext.value, gr.reshape(n, 3), ge.reshape(n, 2), mom
+
+
+# --- Sommerfeld reflected Green's tensor (sommerfeld.rs) ---------------------
+# `somm` is any object with z_interface, wavelength_nm, eps_sub (complex) and
+# eps_env (SubstrateRuntime::Sommerfeld, substrate.rs:109-113).
+
+def somm_bessel(order, x):
+    """J0 / J1 / J2 of sommerfeld.rs:103-153 (the module's own coefficients)."""
+    return lib().orc_somm_bessel(int(order), float(x))
+
+
+def sommerfeld_tensor(somm, ri, rj, nthreads=0):
+    """SommerfeldGreens::evaluate (sommerfeld.rs:254-300) for pairs of points
+    (ri, rj: (P, 3) or (3,)); returns (P, 3, 3) complex (or (3, 3))."""
+    ri = _vec(ri).reshape(-1, 3)
+    rj = _vec(rj).reshape(-1, 3)
+    out = np.zeros((ri.shape[0], 3, 3), np.complex128)
+    s = _somm(somm)
+    lib().orc_sommerfeld_tensor(ctypes.byref(s), ri.shape[0], _p(ri), _p(rj),
+                                _p(out.view(np.float64)), nthreads)
+    return out if out.shape[0] != 1 else out[0]
+
+
+def assemble_sommerfeld(pos, alpha, k, somm, use_fcd=False, cell_size=3.0, lattice=None,
+                        k_bloch=(0, 0, 0), nthreads=0):
+    """assemble_interaction_matrix with the Sommerfeld substrate runtime."""
+    pos = _vec(pos).reshape(-1, 3)
+    n = pos.shape[0]
+    a = _alpha_arr(alpha, n)
+    A = np.zeros((3 * n, 3 * n), np.complex128)
+    s = _somm(somm)
+    rc = lib().orc_assemble_sommerfeld(n, _p(pos), _p(a.view(np.float64)), k, int(use_fcd),
+                                       cell_size, _ref(_lat(lattice)), _p(_vec(k_bloch)),
+                                       ctypes.byref(s), _p(A.view(np.float64)), nthreads)
+    if rc != 0:
+        raise ValueError("singular polarisability")
+    return A
+
+
+def matvec_sommerfeld(pos, alpha, x, k, somm, use_fcd=False, cell_size=3.0, lattice=None,
+                      k_bloch=(0, 0, 0), nthreads=0):
+    """matvec_on_the_fly with the Sommerfeld substrate runtime."""
+    pos = _vec(pos).reshape(-1, 3)
+    n = pos.shape[0]
+    a = _alpha_arr(alpha, n)
+    x = np.ascontiguousarray(np.asarray(x, np.complex128))
+    y = np.zeros(3 * n, np.complex128)
+    s = _somm(somm)
+    rc = lib().orc_matvec_sommerfeld(n, _p(pos), _p(a.view(np.float64)), _p(x.view(np.float64)),
+                                     k, int(use_fcd), cell_size, _ref(_lat(lattice)),
+                                     _p(_vec(k_bloch)), ctypes.byref(s), _p(y.view(np.float64)),
+                                     nthreads)
+    if rc != 0:
+        raise ValueError("singular polarisability")
+    return y
