@@ -387,8 +387,8 @@ class CudaSession:
 
     def kernel_config(self) -> dict:
         """Autotuned kernel choices of this session."""
-        buf = ctypes.create_string_buffer(512)
-        _raise(self._lib.lum_session_kernel_config(self._h, buf, 512), "kernel_config")
+        buf = ctypes.create_string_buffer(1024)
+        _raise(self._lib.lum_session_kernel_config(self._h, buf, 1024), "kernel_config")
         out = {}
         for tok in buf.value.decode().split():
             key, _, val = tok.partition("=")

@@ -93,14 +93,14 @@ lum_status lum_session::apply(int precision, const double2* x, double2* y, const
   }
   if (kind == 0) {
     LUM_TRY(otf.apply(precision, x, y, stream, e0, e1, skip));
-    return otf.somm_apply(x, y, stream, skip);
+    return otf.somm_apply(precision, x, y, stream, skip);
   }
   if (kind == 2) return fft.apply(precision, x, y, stream, e0, e1, skip);
   // cached session
-  if (otf.has_somm && otf.somm_stale) return otf.somm_apply(x, y, stream, skip);  // error
+  if (otf.has_somm && otf.somm_stale) return otf.somm_apply(precision, x, y, stream, skip);
   if (precision == LUM_FP64 && cached.precision == LUM_FP32 && otf.inv_alpha.p) {
     LUM_TRY(otf.apply(LUM_FP64, x, y, stream, nullptr, nullptr, skip));
-    return otf.somm_apply(x, y, stream, skip);
+    return otf.somm_apply(LUM_FP64, x, y, stream, skip);
   }
   if (e0) cudaEventRecord(e0, stream);
   LUM_TRY(cached.apply(x, y, stream, skip));
@@ -132,8 +132,8 @@ lum_status lum_session::apply2(int precision, const double2* x, const double2* x
     e1 = r.b;
   }
   LUM_TRY(otf.apply2(precision, x, x2, y, y2, stream, e0, e1, skip, skip2));
-  LUM_TRY(otf.somm_apply(x, y, stream, skip));
-  return otf.somm_apply(x2, y2, stream, skip2);
+  LUM_TRY(otf.somm_apply(precision, x, y, stream, skip));
+  return otf.somm_apply(precision, x2, y2, stream, skip2);
 }
 
 static bool bad_ptr(const void* p, const char* what) {
@@ -800,12 +800,14 @@ int lum_session_kernel_config(lum_session* s, char* buf, size_t len) {
   snprintf(buf, len,
            "kind=%s f32_variant=%s tuned_ms=%.4f nsplit32=%d nsplit64=%d ell_w=%d lofree=%d "
            "fast_trig=%d f32x2_variant=%s tuned_x2_ms=%.4f nsplit_x2=%d f32_sym=%d "
-           "tuned_sym_ms=%.4f sym_superblocks=%d",
+           "tuned_sym_ms=%.4f sym_superblocks=%d sommerfeld=%s somm_records=%lld",
            s->kind == 0 ? "onthefly" : (s->kind == 1 ? "cached" : "fft"),
            lum::f32_variant_name(o.f32_variant),
            (double)o.tuned_ms, o.nsplit32, o.nsplit64, o.ell_w, o.lofree, o.fast_trig,
            lum::f32x2_variant_name(o.f32x2_variant), (double)o.tuned_x2_ms, o.nsplit_x2,
-           o.f32_sym, (double)o.tuned_sym_ms, o.sym_nb);
+           o.f32_sym, (double)o.tuned_sym_ms, o.sym_nb,
+           o.has_somm ? (o.somm_keyed ? "lattice_keys" : "pairs") : "none",
+           (long long)o.somm_records);
   return LUM_OK;
 }
 

@@ -140,15 +140,26 @@ struct OtfOperator {
   lum_status tune_f32(cudaStream_t st);
   std::vector<double> host_pos;  // double4 host copy (image positions are built from it)
 
-  // Sommerfeld substrate (sommerfeld.cu): the reflected-tensor integrals of
-  // every unordered pair, evaluated once per wavelength into an HBM table of
-  // 64-byte records; each application streams the table (y -= G_refl x).
+  // Sommerfeld substrate (sommerfeld.cu): the reflected-tensor integrals
+  // depend on a pair only through (rho, z_i + z_j).  On a cubic dipole
+  // lattice they are tabulated once per wavelength per key
+  // (da^2 + db^2, c_i + c_j) -- a table of a few MB that stays in L2 -- else
+  // per unordered pair (an HBM table of n(n+1)/2 records).  Records are four
+  // complex values; each application gathers them (y -= G_refl x).
   int has_somm = 0;
   int somm_stale = 0;        // the physics changed after the table was built
   SommDev somm{};
-  DevBuf somm_tab;           // double2 [n(n+1)/2][4]
+  int somm_keyed = 0;        // 1: lattice keys, 0: per unordered pair
+  int somm_T = 0;            // keyed: number of height sums (2 max c + 1)
+  double somm_d = 0.0;       // keyed: lattice pitch
+  double somm_zlo = 0.0;     // keyed: lowest dipole height
+  long long somm_records = 0;
+  DevBuf somm_idx;           // keyed: int4 [n] integer lattice coordinates
+  DevBuf somm_tab;           // double2 [records][4]
+  DevBuf somm_tab32;         // keyed: float2 [records][4]
   lum_status somm_build(const lum_sommerfeld* s, cudaStream_t st);
-  lum_status somm_apply(const double2* x, double2* y, cudaStream_t st, const int* skip) const;
+  lum_status somm_apply(int precision, const double2* x, double2* y, cudaStream_t st,
+                        const int* skip) const;
 
   // Periodic (Ewald) operator on a dipole lattice: every displacement is
   // d*(da, db, dc) with integer steps, so the periodic tensor is tabulated
