@@ -57,14 +57,16 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--workload", default="cuboid",
                    choices=["cuboid", "clusters", "dimer", "metasurface", "cached", "fields",
-                            "fft", "directions"],
+                            "fft", "directions", "sommerfeld", "harmonic"],
                    help="cuboid: the headline N=30k solve; clusters: 256 Drude ellipsoids x 2 "
                         "polarisations in one batch; dimer: helix-dimer adjoint gradients; "
                         "metasurface: periodic Ewald + substrate sweep; cached: the assembled "
                         "3N x 3N matrix, single-vector GEMV and multi-RHS tensor-core product; "
                         "fields: near-field map and far field from solved moments; fft: the "
                         "headline cuboid through the block-Toeplitz FFT operator; directions: "
-                        "many incidence directions of one cached matrix on the tensor cores")
+                        "many incidence directions of one cached matrix on the tensor cores; "
+                        "sommerfeld: an Au sphere above glass with the Sommerfeld substrate; "
+                        "harmonic: second-harmonic response of the headline cuboid")
     p.add_argument("--nrhs", type=int, default=128, help="right-hand sides (cached workload)")
     p.add_argument("--clusters", type=int, default=256)
     p.add_argument("--spacing", type=float, default=None)
@@ -467,6 +469,10 @@ def run_secondary(args):
             line = _bench_fft(args, bk, stream, torch, lb, configs)
         elif args.workload == "fields":
             line = _bench_fields(args, bk, stream, torch, lb, configs, fp64_peak)
+        elif args.workload == "sommerfeld":
+            line = _bench_sommerfeld(args, bk, stream, torch, lb, configs, fp32_peak)
+        elif args.workload == "harmonic":
+            line = _bench_harmonic(args, bk, stream, torch, lb, configs)
         else:
             line = _bench_metasurface(args, bk, stream, torch, lb, configs)
     line["gpu_launches"] = _ffi.launch_count() - launches0
@@ -906,6 +912,173 @@ def _bench_fields(args, bk, stream, torch, lb, configs, fp64_peak):
                                  "the host<->device copies; FP64 FMA-chain peak; of measured"},
             "e2e": {"value": pn / tn, "unit": "pairs/s", "h2d_bytes_per_step": n * (24 + 48),
                     "d2h_bytes_per_step": 256 * 256 * 8}}
+
+
+SOMM_FLOPS_PER_PAIR = 100.0  # block from a record (24) + 3x3 complex product (72) + rho, cos/sin
+
+
+def _bench_sommerfeld(args, bk, stream, torch, lb, configs, fp32_peak):
+    """An Au sphere (R = 30 nm, 2 nm lattice, N = 14,147) 5 nm above glass
+    (eps 2.25) in air at 520 nm with the Sommerfeld substrate (sommerfeld.rs,
+    SubstrateRuntime::Sommerfeld): session set-up including the reflected-
+    integral table, FP32+refine and FP64 GMRES(30) solves at tol 1e-8 with C_ext
+    compared, one operator application per precision, and the host oracle's
+    reflected-tensor cost per pair scaled to the reference's on-the-fly solve,
+    which re-evaluates G_refl for every ordered pair of every matvec."""
+    from lumina_b200.geometry import Sphere, discretise_primitive
+    from lumina_b200.lattice import SommerfeldRuntime
+    radius, gap, lam = 30.0, 5.0, 520.0
+    pos = discretise_primitive(Sphere((0.0, 0.0, 0.0), radius), 2.0).copy()
+    pos[:, 2] += radius + gap
+    w = configs.au_workload("sphere_on_glass", pos, 2.0, lam)
+    n = w.n
+    inv = lb.invert_polarisability(w.alpha)
+    somm = SommerfeldRuntime(0.0, lam, 2.25 + 0.0j, 1.0)
+    rhs = lb.incident_field(w.positions, w.k, lb.IncidentField())
+    tol, max_iter = 1e-8, max(args.max_iter, 20000)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    S = bk.create_onthefly_session(w.positions, inv, w.k, True, 2.0, substrate=somm)
+    setup_ms = (time.perf_counter() - t0) * 1e3
+    S.set_stream(stream.cuda_stream)
+    b_dev = torch.from_numpy(rhs).to("cuda")
+    x_dev = torch.zeros_like(b_dev)
+    for _ in range(args.warmup):
+        for mode in ("fp32_refine", "fp64"):
+            try:
+                S.solve_device(b_dev.data_ptr(), x_dev.data_ptr(), tol, 31, 30, mode,
+                               stream.cuda_stream)
+            except lb.ConvergenceFailure:
+                pass
+    flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")
+    t32 = []
+    for _ in range(max(args.steps, 1)):
+        flush.zero_()
+        info32, ms = _timed(stream, lambda: S.solve_device(b_dev.data_ptr(), x_dev.data_ptr(), tol,
+                                                           max_iter, 30, "fp32_refine",
+                                                           stream.cuda_stream))
+        t32.append(ms)
+    x32 = x_dev.cpu().numpy()
+    c32 = lb.cross_sections(w.positions, inv, x32, w.k, lb.IncidentField())[0]
+    info64, ms64, c64 = info32, float("nan"), c32
+    if not args.no_fp64:
+        flush.zero_()
+        info64, ms64 = _timed(stream, lambda: S.solve_device(b_dev.data_ptr(), x_dev.data_ptr(),
+                                                             tol, max_iter, 30, "fp64",
+                                                             stream.cuda_stream))
+        x64 = x_dev.cpu().numpy()
+        c64 = lb.cross_sections(w.positions, inv, x64, w.k, lb.IncidentField())[0]
+    xr = torch.randn(3 * n, dtype=torch.complex128, device="cuda")
+    yr = torch.empty_like(xr)
+    apply_ms = {}
+    for prec in ("fp32", "fp64"):
+        for _ in range(3):
+            S.matvec_device(xr.data_ptr(), yr.data_ptr(), prec, stream.cuda_stream)
+        _, ms = _timed(stream, lambda: [S.matvec_device(xr.data_ptr(), yr.data_ptr(), prec,
+                                                        stream.cuda_stream) for _ in range(20)])
+        apply_ms[prec] = ms / 20
+    # end to end through the public host-array call (copies included)
+    e2e_s = float("nan")
+    if not args.no_e2e:
+        t0 = time.perf_counter()
+        S.solve(rhs, tol, max_iter, 30, "fp32_refine")
+        e2e_s = time.perf_counter() - t0
+    cfg = S.kernel_config()
+    S.close()
+    ms32 = statistics.median(t32)
+    line = {"metric": "dipole-solves/s, Au sphere above glass with the Sommerfeld substrate, "
+                      "FP32+refine", "value": n / (ms32 * 1e-3), "unit": UNIT,
+            "higher_is_better": True, "steps": len(t32), "ms_per_step": ms32, "scaling": "weak",
+            "dtype": "f32+f64", "mode": "fp32_refine",
+            "config": {"workload": "Au sphere R = 30 nm, 2 nm lattice, 5 nm above glass "
+                                   "(eps 2.25) in air, 520 nm, FCD, Sommerfeld substrate, "
+                                   "GMRES(30) tol 1e-8", "n_dipoles": n,
+                       "l2": "64 MB flush before each timed solve"},
+            "setup_ms": setup_ms, "iterations": info32["iterations"],
+            "iterations_fp64": info64["iterations"], "converged": bool(info32["converged"]),
+            "fp64_plain": None if args.no_fp64 else {"value": n / (ms64 * 1e-3), "ms": ms64,
+                                                     "speedup_same_solves": ms64 / ms32},
+            "cext_rel_err_fp32_refine_vs_fp64": None if args.no_fp64 else abs(c32 - c64) / abs(c64),
+            "apply_ms": apply_ms, "kernel_config": cfg,
+            "e2e": None if args.no_e2e else {"value": n / e2e_s, "unit": UNIT,
+                                             "h2d_bytes_per_step": rhs.nbytes,
+                                             "d2h_bytes_per_step": rhs.nbytes}}
+    pairs = float(n) * n
+    achieved = pairs * SOMM_FLOPS_PER_PAIR / (apply_ms["fp32"] * 1e-3) / 1e12
+    line["roofline"] = {"bound": "fp32", "kernel": "somm_apply_rows<float> + free-space pairs",
+                        "achieved": achieved, "peak": fp32_peak / 1e3, "unit": "TFLOP/s",
+                        "frac": achieved / (fp32_peak / 1e3),
+                        "note": "lower bound: the whole FP32 application timed, only the "
+                                "reflected term's ~100 flops per ordered pair counted; FP32 "
+                                "FMA-chain peak; of measured"}
+    if not args.no_cpu:
+        from oracle import oracle as orc
+        nt = orc.max_threads()
+        rng = np.random.default_rng(5)
+        m = 512
+        dt = 0.0
+        while True:
+            ii, jj = rng.integers(0, n, m), rng.integers(0, n, m)
+            t0 = time.perf_counter()
+            orc.sommerfeld_tensor(somm, w.positions[ii], w.positions[jj], nt)
+            dt = time.perf_counter() - t0
+            if dt > min(args.cpu_seconds, 10.0) / 4 or m >= (1 << 22):
+                break
+            m *= 4
+        t_pair = dt / m
+        mv_ref = int(info64.get("matvecs_reference", info64["iterations"]))
+        t_solve = t_pair * pairs * mv_ref
+        line["cpu_baseline"] = {"value": n / t_solve, "unit": UNIT, "cores": nt, "kind": "port",
+                                "sample": f"{m} random pairs of the reflected tensor "
+                                          f"({dt:.1f} s), scaled to N^2 pairs per matvec x "
+                                          f"{mv_ref} matvecs of the FP64 solve (free-space "
+                                          f"term not counted: a lower bound on the "
+                                          f"reference's time)", "cpu": _cpu_model()}
+    return line
+
+
+def _bench_harmonic(args, bk, stream, torch, lb, configs):
+    """Second-harmonic response (nonlinear.rs:108-240) of the headline cuboid
+    (60x50x10 nm Au, N = 30,000, FCD cell 1 nm): the linear FP32+refine solve
+    at 800 nm (untimed), then compute_shg_response at 400 nm -- chi(2)
+    sources from the local fields on the device and the harmonic GMRES(30)
+    solve at tol 1e-8 through the solver's session dispatch (matrix-free at
+    this size) -- timed end to end through the public call with host arrays."""
+    from lumina_b200 import nonlinear
+    w1 = configs.cuboid_au_30k(800.0)
+    w2 = configs.cuboid_au_30k(400.0)
+    n = w1.n
+    solver = lb.CdaSolver(iterative_threshold=1000, use_fcd=True, cell_size=1.0, backend=bk,
+                          precision="fp32_refine")
+    params = lb.SimulationParams(solver_tolerance=1e-8, max_iterations=max(args.max_iter, 20000))
+    resp = solver.solve_dipoles(lb.DipoleSet(w1.positions, w1.alpha), 800.0, params)
+    d2 = lb.DipoleSet(w2.positions, w2.alpha)
+    chi2 = [nonlinear.Chi2Tensor.isotropic_surface(1.0 + 0.2j, 0.4)]
+    for _ in range(max(args.warmup, 1)):
+        nonlinear.compute_shg_response(solver, resp, d2, chi2, params)
+    times, r = [], None
+    for _ in range(max(args.steps, 1)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = nonlinear.compute_shg_response(solver, resp, d2, chi2, params)
+        times.append(time.perf_counter() - t0)
+    t = statistics.median(times)
+    info = r.solve_info
+    line = {"metric": "dipole-solves/s, second-harmonic response of the N=30k cuboid "
+                      "(sources + harmonic solve, FP32+refine)", "value": n / t, "unit": UNIT,
+            "higher_is_better": True, "steps": len(times), "ms_per_step": t * 1e3,
+            "scaling": "weak", "dtype": "f32+f64", "mode": "fp32_refine",
+            "config": {"workload": "Au cuboid 60x50x10 nm (N=30,000), FCD 1 nm, fundamental "
+                                   "800 nm, SHG at 400 nm, isotropic-surface chi(2), "
+                                   "GMRES(30) tol 1e-8", "n_dipoles": n},
+            "iterations": info.get("iterations"), "converged": bool(info.get("converged")),
+            "shg_intensity": r.intensity,
+            "e2e": {"value": n / t, "unit": UNIT, "h2d_bytes_per_step": n * (24 + 144 + 48),
+                    "d2h_bytes_per_step": n * 48}}
+    if not args.no_cpu:
+        mv = int(info.get("matvecs_reference") or info.get("iterations") or 1)
+        line["cpu_baseline"] = cpu_baseline(w2, mv, args.cpu_seconds)
+    return line
 
 
 def _bench_metasurface(args, bk, stream, torch, lb, configs):

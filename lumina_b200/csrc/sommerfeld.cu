@@ -369,6 +369,107 @@ somm_apply_rows(int n, const double4* __restrict__ pos, SommIdx K,
     }
 }
 
+// Lattice-keyed application: the block's eight rows share column tiles of
+// lattice coordinates and x staged in shared memory; cos phi and sin phi come
+// from the integer offsets (da, db) / sqrt(s), so a pair reads only its
+// record (from L2) beyond the tile.
+constexpr int kSommTile = 128;
+template <typename R>
+__global__ void __launch_bounds__(32 * kSommRows)
+somm_apply_keyed(int n, const int4* __restrict__ lidx, int T,
+                 const typename SommT<R>::R2* __restrict__ tab, const double2* __restrict__ x,
+                 double2* __restrict__ y, const int* __restrict__ skip) {
+  typedef typename SommT<R>::R2 R2;
+  __shared__ int4 s_l[kSommTile];
+  __shared__ R2 s_x[3][kSommTile];
+  if (skip && *skip) return;  // the flag is the same for the whole block
+  const int i = blockIdx.x * kSommRows + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  const bool active = i < n;
+  const int4 li = active ? lidx[i] : make_int4(0, 0, 0, 0);
+  R2 acc[3];
+  for (int a = 0; a < 3; ++a) acc[a] = SommT<R>::mk(R(0), R(0));
+  for (int c0 = 0; c0 < n; c0 += kSommTile) {
+    __syncthreads();
+    if (threadIdx.x < kSommTile) {
+      const int t = threadIdx.x, j = c0 + t;
+      if (j < n) {
+        s_l[t] = lidx[j];
+        for (int c = 0; c < 3; ++c) {
+          const double2 v = x[3 * (size_t)j + c];
+          s_x[c][t] = SommT<R>::mk((R)v.x, (R)v.y);
+        }
+      }
+    }
+    __syncthreads();
+    const int cmax = min(kSommTile, n - c0);
+    if (active) {
+#pragma unroll 2
+      for (int t = lane; t < cmax; t += 32) {
+        const int4 lj = s_l[t];
+        const int da = li.x - lj.x, db = li.y - lj.y;
+        const int sq = da * da + db * db;
+        const R2* rec = tab + kSommRecordC * ((size_t)sq * T + (size_t)(li.z + lj.z));
+        R2 A, B, Z, X;
+        if constexpr (sizeof(R) == 4) {
+          const float4 r0 = __ldg(reinterpret_cast<const float4*>(rec));
+          const float4 r1 = __ldg(reinterpret_cast<const float4*>(rec) + 1);
+          A = SommT<R>::mk(r0.x, r0.y);
+          B = SommT<R>::mk(r0.z, r0.w);
+          Z = SommT<R>::mk(r1.x, r1.y);
+          X = SommT<R>::mk(r1.z, r1.w);
+        } else {
+          A = __ldg(rec);
+          B = __ldg(rec + 1);
+          Z = __ldg(rec + 2);
+          X = __ldg(rec + 3);
+        }
+        R cp = R(1), sp = R(0);
+        if (sq > 0) {
+          const R inv = rsqrt((R)sq);
+          cp = (R)da * inv;
+          sp = (R)db * inv;
+        }
+        const R c2 = R(2) * cp * cp - R(1), s2 = R(2) * sp * cp;
+        const R2 gxx = SommT<R>::mk(A.x - B.x * c2, A.y - B.y * c2);
+        const R2 gyy = SommT<R>::mk(A.x + B.x * c2, A.y + B.y * c2);
+        const R2 gxy = SommT<R>::mk(-B.x * s2, -B.y * s2);
+        const R2 gxz = SommT<R>::mk(X.x * cp, X.y * cp);
+        const R2 gyz = SommT<R>::mk(X.x * sp, X.y * sp);
+        const R2 x0 = s_x[0][t], x1 = s_x[1][t], x2 = s_x[2][t];
+        acc[0].x += gxx.x * x0.x - gxx.y * x0.y + gxy.x * x1.x - gxy.y * x1.y + gxz.x * x2.x -
+                    gxz.y * x2.y;
+        acc[0].y += gxx.x * x0.y + gxx.y * x0.x + gxy.x * x1.y + gxy.y * x1.x + gxz.x * x2.y +
+                    gxz.y * x2.x;
+        acc[1].x += gxy.x * x0.x - gxy.y * x0.y + gyy.x * x1.x - gyy.y * x1.y + gyz.x * x2.x -
+                    gyz.y * x2.y;
+        acc[1].y += gxy.x * x0.y + gxy.y * x0.x + gyy.x * x1.y + gyy.y * x1.x + gyz.x * x2.y +
+                    gyz.y * x2.x;
+        acc[2].x += gxz.x * x0.x - gxz.y * x0.y + gyz.x * x1.x - gyz.y * x1.y - Z.x * x2.x +
+                    Z.y * x2.y;
+        acc[2].y += gxz.x * x0.y + gxz.y * x0.x + gyz.x * x1.y + gyz.y * x1.x - Z.x * x2.y -
+                    Z.y * x2.x;
+      }
+    }
+  }
+  if (!active) return;
+  double ax[3], ay[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    ax[a] = (double)acc[a].x;
+    ay[a] = (double)acc[a].y;
+    for (int o = 16; o > 0; o >>= 1) {
+      ax[a] += __shfl_xor_sync(0xffffffffu, ax[a], o);
+      ay[a] += __shfl_xor_sync(0xffffffffu, ay[a], o);
+    }
+  }
+  if (lane == 0)
+    for (int a = 0; a < 3; ++a) {
+      double2& e = y[3 * (size_t)i + a];
+      e = make_double2(e.x - ax[a], e.y - ay[a]);
+    }
+}
+
 template <typename T2> __device__ __forceinline__ T2 somm_mk(double re, double im);
 template <> __device__ __forceinline__ float2 somm_mk<float2>(double re, double im) {
   return make_float2((float)re, (float)im);
@@ -601,9 +702,12 @@ lum_status OtfOperator::somm_apply(int precision, const double2* x, double2* y, 
   }
   const SommIdx K = somm_indexer(*this);
   const unsigned blocks = (unsigned)((n + kSommRows - 1) / kSommRows);
-  if (precision == LUM_FP32 && somm_keyed)
-    somm_apply_rows<float><<<blocks, 32 * kSommRows, 0, st>>>(
-        n, pos64.as<double4>(), K, somm_tab32.as<float2>(), x, y, skip);
+  if (somm_keyed && precision == LUM_FP32)
+    somm_apply_keyed<float><<<blocks, 32 * kSommRows, 0, st>>>(
+        n, somm_idx.as<int4>(), somm_T, somm_tab32.as<float2>(), x, y, skip);
+  else if (somm_keyed)
+    somm_apply_keyed<double><<<blocks, 32 * kSommRows, 0, st>>>(
+        n, somm_idx.as<int4>(), somm_T, somm_tab.as<double2>(), x, y, skip);
   else
     somm_apply_rows<double><<<blocks, 32 * kSommRows, 0, st>>>(
         n, pos64.as<double4>(), K, somm_tab.as<double2>(), x, y, skip);
