@@ -985,6 +985,29 @@ def _bench_sommerfeld(args, bk, stream, torch, lb, configs, fp32_peak):
         e2e_s = time.perf_counter() - t0
     cfg = S.kernel_config()
     S.close()
+    # the same system through the FFT operator: the reflected term as a second
+    # convolution in the z-mirrored coordinate
+    F = bk.create_fft_session(w.positions, inv, w.k, True, 2.0, substrate=somm)
+    F.set_stream(stream.cuda_stream)
+    for _ in range(args.warmup):
+        try:
+            F.solve_device(b_dev.data_ptr(), x_dev.data_ptr(), tol, 31, 30, "fp32_refine",
+                           stream.cuda_stream)
+        except lb.ConvergenceFailure:
+            pass
+    flush.zero_()
+    infof, msf = _timed(stream, lambda: F.solve_device(b_dev.data_ptr(), x_dev.data_ptr(), tol,
+                                                       max_iter, 30, "fp32_refine",
+                                                       stream.cuda_stream))
+    cf = lb.cross_sections(w.positions, inv, x_dev.cpu().numpy(), w.k, lb.IncidentField())[0]
+    fft_apply = {}
+    for prec in ("fp32", "fp64"):
+        for _ in range(3):
+            F.matvec_device(xr.data_ptr(), yr.data_ptr(), prec, stream.cuda_stream)
+        _, ms = _timed(stream, lambda: [F.matvec_device(xr.data_ptr(), yr.data_ptr(), prec,
+                                                        stream.cuda_stream) for _ in range(20)])
+        fft_apply[prec] = ms / 20
+    F.close()
     ms32 = statistics.median(t32)
     line = {"metric": "dipole-solves/s, Au sphere above glass with the Sommerfeld substrate, "
                       "FP32+refine", "value": n / (ms32 * 1e-3), "unit": UNIT,
@@ -1000,6 +1023,9 @@ def _bench_sommerfeld(args, bk, stream, torch, lb, configs, fp32_peak):
                                                      "speedup_same_solves": ms64 / ms32},
             "cext_rel_err_fp32_refine_vs_fp64": None if args.no_fp64 else abs(c32 - c64) / abs(c64),
             "apply_ms": apply_ms, "kernel_config": cfg,
+            "fft_operator": {"value": n / (msf * 1e-3), "ms": msf,
+                             "iterations": infof["iterations"], "apply_ms": fft_apply,
+                             "cext_rel_err_vs_onthefly": abs(cf - c32) / abs(c32)},
             "e2e": None if args.no_e2e else {"value": n / e2e_s, "unit": UNIT,
                                              "h2d_bytes_per_step": rhs.nbytes,
                                              "d2h_bytes_per_step": rhs.nbytes}}

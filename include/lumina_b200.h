@@ -163,8 +163,13 @@ LUM_API int lum_session_create_onthefly(lum_ctx* ctx, int n_dipoles, const doubl
  * cubic lattice (empty nodes hold zero), not only a full box.  `spacing` is
  * the lattice pitch (<= 0: cell_size, as detect_regular_grid takes it,
  * fft_matvec.rs:19); every dipole must lie within 1e-6 spacing of a node,
- * at most 512 nodes per axis, no lattice sum, no substrate.  The session
- * supports matvec, the solves and set_wavelength. */
+ * at most 512 nodes per axis, no lattice sum.  The session supports matvec,
+ * the solves and set_wavelength.  A planar substrate is added as a second
+ * convolution in the z-mirrored coordinate (six more spectra, no further FFT
+ * per product): the Fresnel image term through lum_session_set_wavelength's
+ * substrate argument, the Sommerfeld term through lum_session_set_sommerfeld.
+ * Neither is in the reference's FFT plan, which declines substrates
+ * (cda/mod.rs:286-298). */
 LUM_API int lum_session_create_fft(lum_ctx* ctx, int n_dipoles, const double* pos,
                                    const double* inv_alpha, double k, int use_fcd,
                                    double cell_size, double spacing, lum_session** out);
@@ -196,8 +201,9 @@ LUM_API int lum_session_create_onthefly_sommerfeld(lum_ctx* ctx, int n_dipoles,
                                                    lum_session** out);
 /* Rebuilds the Sommerfeld table of an on-the-fly session for new substrate
  * parameters (after lum_session_set_wavelength, which marks the table stale:
- * until it is rebuilt the session's applications fail with INVALID), or
- * re-assembles a cached session's matrix with them. */
+ * until it is rebuilt the session's applications fail with INVALID),
+ * re-assembles a cached session's matrix with them, or builds an FFT
+ * session's reflected spectra. */
 LUM_API int lum_session_set_sommerfeld(lum_session* s, const lum_sommerfeld* somm);
 /* SommerfeldGreens::evaluate (sommerfeld.rs:254-300) on the device for
  * npairs point pairs: ri, rj are npairs x 3, g receives npairs x 3 x 3

@@ -569,9 +569,10 @@ class CudaBackend:
         return CudaSession(h, 3 * n, "cached", self)
 
     def create_fft_session(self, positions, inv_alpha, k: float, use_fcd=True,
-                           cell_size=3.0, spacing=0.0) -> CudaSession:
+                           cell_size=3.0, spacing=0.0, substrate=None) -> CudaSession:
         """Block-Toeplitz session through 3D FFTs (fft_matvec.rs:77-258, widened
-        to FCD and to any set of cubic-lattice nodes)."""
+        to FCD, to any set of cubic-lattice nodes and to a planar substrate --
+        a SubstrateRuntime (Fresnel image) or a SommerfeldRuntime)."""
         pos = np.ascontiguousarray(np.asarray(positions, np.float64).reshape(-1, 3))
         n = pos.shape[0]
         ia = _c128(inv_alpha, 9 * n)
@@ -579,7 +580,17 @@ class CudaBackend:
         _raise(self._lib.lum_session_create_fft(self._h, n, _dp(pos), _dp(ia.view(np.float64)),
                                                 float(k), int(bool(use_fcd)), float(cell_size),
                                                 float(spacing), byref(h)), "create_fft_session")
-        return CudaSession(h, 3 * n, "fft", self)
+        sess = CudaSession(h, 3 * n, "fft", self)
+        if substrate is not None:
+            try:
+                if _is_sommerfeld(substrate):
+                    sess.set_sommerfeld(substrate)
+                else:
+                    sess.set_wavelength(k, ia, substrate)
+            except Exception:
+                sess.close()
+                raise
+        return sess
 
     def create_onthefly_session(self, positions, inv_alpha, k: float, use_fcd=True,
                                 cell_size=3.0, lattice=None, k_bloch=(0.0, 0.0, 0.0),

@@ -422,13 +422,20 @@ int lum_session_set_wavelength(lum_session* s, double k, const double* inv_alpha
                                const lum_substrate* substrate) {
   if (bad_ptr(s, "session")) return LUM_ERR_INVALID;
   if (s->kind == 2) {
-    if (substrate) {
-      set_error("the FFT operator has no substrate term");
+    LUM_TRY(check_physics(s->n_dipoles, inv_alpha, k));
+    if (substrate && s->fft.refl_mode == 2) {
+      set_error("a Sommerfeld session takes no Fresnel substrate");
       return LUM_ERR_INVALID;
     }
-    LUM_TRY(check_physics(s->n_dipoles, inv_alpha, k));
     cudaSetDevice(s->ctx->device);
-    return s->fft.set_physics(k, inv_alpha, s->stream);
+    LUM_TRY(s->fft.set_physics(k, inv_alpha, s->stream));
+    // the reflected spectra: Fresnel rebuilt here, Sommerfeld waits for
+    // lum_session_set_sommerfeld
+    if (substrate) LUM_TRY(s->fft.set_reflection(1, substrate, nullptr, s->stream));
+    else if (s->fft.refl_mode == 2) s->fft.refl_stale = 1;
+    else if (s->fft.refl_mode == 1) LUM_TRY(s->fft.set_reflection(0, nullptr, nullptr, s->stream));
+    LUM_TRY_CUDA(cudaStreamSynchronize(s->stream));
+    return LUM_OK;
   }
   if (!s->otf.inv_alpha.p) {
     set_error("set_wavelength needs a geometry session");
@@ -558,7 +565,19 @@ int lum_session_assemble_sommerfeld(lum_ctx* ctx, int n, const double* pos,
 
 int lum_session_set_sommerfeld(lum_session* s, const lum_sommerfeld* somm) {
   if (bad_ptr(s, "session") || bad_ptr(somm, "somm")) return LUM_ERR_INVALID;
-  if (s->kind == 2 || !s->otf.inv_alpha.p) {
+  if (s->kind == 2) {
+    if (s->fft.refl_mode == 1) {
+      set_error("the session already has a Fresnel substrate");
+      return LUM_ERR_INVALID;
+    }
+    lum::SommDev S;
+    LUM_TRY(lum::somm_params(somm, &S));
+    cudaSetDevice(s->ctx->device);
+    LUM_TRY(s->fft.set_reflection(2, nullptr, &S, s->stream));
+    LUM_TRY_CUDA(cudaStreamSynchronize(s->stream));
+    return LUM_OK;
+  }
+  if (!s->otf.inv_alpha.p) {
     set_error("the Sommerfeld substrate needs an on-the-fly or assembled session");
     return LUM_ERR_INVALID;
   }

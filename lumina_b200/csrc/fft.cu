@@ -18,6 +18,15 @@
 // Padded dimensions are powers of two >= 2 n - 1 per axis.  The tensor is
 // symmetric (greens.rs:34-71), so six kernel spectra are stored.
 //
+// A planar substrate adds R(r_i, r_j), a function of (x_i - x_j, y_i - y_j,
+// z_i + z_j): the Fresnel image tensor G(r_i - rbar_j) with column factors m
+// (assembly.rs:129-156, :274-295) or the Sommerfeld G_refl (sommerfeld.rs).
+// With c' = -c_j it is a convolution in the z-mirrored coordinate: on the
+// circulant, x~(c) = x(-c mod Mz) has the spectrum X(kx, ky, -kz), so the
+// reflected term is R^(k) . (m o X)(kx, ky, -kz) -- six more spectra and no
+// further FFT.  The table holds R at height sums t = c + c' in [0, 2 n_z - 2]
+// and lateral displacements as for G.
+//
 // FFTs are hand-written: batched radix-2 Stockham passes (the autosort
 // formulation of Govindaraju et al., "High Performance Discrete Fourier
 // Transforms on Graphics Processors", SC 2008) along one axis at a time,
@@ -27,8 +36,7 @@
 // FP64 and FP32 variants: the FP32 product (FP32 FFTs against FP32 copies
 // of the FP64 kernel spectra) is the refinement inner operator, the FP64
 // one the residual operator.
-#include "lumina_internal.cuh"
-#include "device_physics.cuh"
+#include "sommerfeld.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -179,6 +187,51 @@ __global__ void fft_spectral_product(size_t mtot, const typename Cx<R>::T* __res
   }
 }
 
+// With a substrate: Y(k) = K(k) X(k) + R(k) (m o X)(kx, ky, -kz).  One thread
+// takes the frequency pair (kz, Mz - kz) of a (kx, ky) line, so both inputs
+// are read before either output is written.
+template <typename R>
+__global__ void fft_spectral_product_refl(int lines, int mz, size_t mtot,
+                                          const typename Cx<R>::T* __restrict__ kern,
+                                          const typename Cx<R>::T* __restrict__ refl,
+                                          typename Cx<R>::T m0, typename Cx<R>::T m1,
+                                          typename Cx<R>::T m2,
+                                          typename Cx<R>::T* __restrict__ buf,
+                                          const int* __restrict__ skip) {
+  using T2 = typename Cx<R>::T;
+  if (skip && *skip) return;
+  const int half = mz / 2 + 1;
+  const size_t count = (size_t)lines * half;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < count;
+       q += (size_t)gridDim.x * blockDim.x) {
+    const size_t line = q / half;
+    const int nz = (int)(q % half);
+    const int nz2 = (mz - nz) % mz;
+    const size_t g[2] = {line * mz + nz, line * mz + nz2};
+    const int cnt = (nz2 == nz) ? 1 : 2;
+    T2 X[2][3];
+    for (int h = 0; h < cnt; ++h)
+      for (int c = 0; c < 3; ++c) X[h][c] = buf[c * mtot + g[h]];
+    for (int h = 0; h < cnt; ++h) {
+      const size_t gg = g[h];
+      const int o = (cnt == 2) ? 1 - h : 0;   // the mirrored frequency
+      const T2 xm[3] = {cmulT(m0, X[o][0]), cmulT(m1, X[o][1]), cmulT(m2, X[o][2])};
+      const T2 kxx = kern[gg], kxy = kern[mtot + gg], kxz = kern[2 * mtot + gg];
+      const T2 kyy = kern[3 * mtot + gg], kyz = kern[4 * mtot + gg], kzz = kern[5 * mtot + gg];
+      const T2 rxx = refl[gg], rxy = refl[mtot + gg], rxz = refl[2 * mtot + gg];
+      const T2 ryy = refl[3 * mtot + gg], ryz = refl[4 * mtot + gg], rzz = refl[5 * mtot + gg];
+      const T2* x = X[h];
+      buf[gg] = cadd(cadd(cadd(cmulT(kxx, x[0]), cmulT(kxy, x[1])), cmulT(kxz, x[2])),
+                     cadd(cadd(cmulT(rxx, xm[0]), cmulT(rxy, xm[1])), cmulT(rxz, xm[2])));
+      buf[mtot + gg] = cadd(cadd(cadd(cmulT(kxy, x[0]), cmulT(kyy, x[1])), cmulT(kyz, x[2])),
+                            cadd(cadd(cmulT(rxy, xm[0]), cmulT(ryy, xm[1])), cmulT(ryz, xm[2])));
+      buf[2 * mtot + gg] =
+          cadd(cadd(cadd(cmulT(kxz, x[0]), cmulT(kyz, x[1])), cmulT(kzz, x[2])),
+               cadd(cadd(cmulT(rxz, xm[0]), cmulT(ryz, xm[1])), cmulT(rzz, xm[2])));
+    }
+  }
+}
+
 // y_i = alpha_i^-1 x_i - (G x)_i, (G x)_i = buf[.][grid_of[i]] / mtot (FP64).
 template <typename R>
 __global__ void fft_gather(int n, size_t mtot, const int* __restrict__ grid_of,
@@ -259,6 +312,57 @@ __global__ void fft_kernel_table(int mx, int my, int mz, int gx, int gy, int gz,
           }
       } else {
         greens_point_d(dx, dy, dz, k, t);
+      }
+    }
+    const int sym[6] = {0, 1, 2, 4, 5, 8};  // xx xy xz yy yz zz
+    for (int c = 0; c < 6; ++c) kern[c * mtot + g] = t[sym[c]];
+  }
+}
+
+// Reflected table: R at lateral displacement (dl, dm) and height sum t = nn
+// (zero for t > 2 gz - 2).  mode 1: the Fresnel image tensor
+// G(dl d, dm d, 2 (z_lo - z0) + t d), skipped below r^2 = 1e-20
+// (assembly.rs:129-156); mode 2: the Sommerfeld G_refl with rho = d |(dl, dm)|,
+// dz = 2 (z_lo - z0) + t d, zero for dz <= 0 (sommerfeld.rs:254-300).
+__global__ void fft_refl_table(int mx, int my, int mz, int gx, int gy, int gz, double spacing,
+                               double zlo, double z0, int mode, double k, SommDev S,
+                               double2* __restrict__ kern) {
+  const size_t mtot = (size_t)mx * my * mz;
+  for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < mtot;
+       g += (size_t)gridDim.x * blockDim.x) {
+    const int l = (int)(g / ((size_t)my * mz)), m = (int)((g / mz) % my), nn = (int)(g % mz);
+    auto disp = [](int v, int M, int n, bool& ok) {
+      if (v <= n - 1) return v;
+      if (v >= M - (n - 1)) return v - M;
+      ok = false;
+      return 0;
+    };
+    bool ok = nn <= 2 * gz - 2;
+    const int dl = disp(l, mx, gx, ok), dm = disp(m, my, gy, ok);
+    double2 t[9];
+    for (int e = 0; e < 9; ++e) t[e] = make_double2(0.0, 0.0);
+    if (ok) {
+      const double dx = dl * spacing, dy = dm * spacing;
+      const double dz = (zlo - z0) + (zlo - z0) + nn * spacing;
+      if (mode == 1) {
+        if (dx * dx + dy * dy + dz * dz >= 1e-20) greens_point_d(dx, dy, dz, k, t);
+      } else if (dz > 0.0) {
+        const int sq = dl * dl + dm * dm;
+        double2 v[4];
+        somm_record(somm_integrals(S, spacing * sqrt((double)sq), dz), v);
+        double cp = 1.0, sp = 0.0;
+        if (sq > 0) {
+          const double inv = rsqrt((double)sq);
+          cp = dl * inv;
+          sp = dm * inv;
+        }
+        const double c2 = 2.0 * cp * cp - 1.0, s2 = 2.0 * sp * cp;
+        t[0] = make_double2(v[0].x - v[1].x * c2, v[0].y - v[1].y * c2);
+        t[4] = make_double2(v[0].x + v[1].x * c2, v[0].y + v[1].y * c2);
+        t[8] = make_double2(-v[2].x, -v[2].y);
+        t[1] = make_double2(-v[1].x * s2, -v[1].y * s2);
+        t[2] = make_double2(v[3].x * cp, v[3].y * cp);
+        t[5] = make_double2(v[3].x * sp, v[3].y * sp);
       }
     }
     const int sym[6] = {0, 1, 2, 4, 5, 8};  // xx xy xz yy yz zz
@@ -372,6 +476,7 @@ lum_status FftOperator::build(const double* pos_host, int n_, double spacing_, d
       node[3 * (size_t)i + c] = (int)r;
       hi[c] = std::max(hi[c], (int)r);
     }
+  lo_z = lo[2];
   for (int c = 0; c < 3; ++c) {
     gn[c] = hi[c] + 1;
     M[c] = 1;
@@ -451,10 +556,48 @@ lum_status FftOperator::set_physics(double k_, const double* inv_alpha_host, cud
   return LUM_OK;
 }
 
+lum_status FftOperator::set_reflection(int mode, const lum_substrate* fresnel,
+                                      const SommDev* somm, cudaStream_t st) {
+  refl_mode = mode;
+  refl_stale = 0;
+  if (mode == 0) {
+    refl64.release();
+    refl32.release();
+    return LUM_OK;
+  }
+  SommDev S{};
+  double z0 = 0.0;
+  if (mode == 1) {
+    z0 = fresnel->z_interface;
+    const double2 r = make_double2(fresnel->refl_re, fresnel->refl_im);
+    refl_m[0] = make_double2(-r.x, -r.y);
+    refl_m[1] = make_double2(-r.x, -r.y);
+    refl_m[2] = r;
+  } else {
+    S = *somm;
+    z0 = S.z0;
+    for (int c = 0; c < 3; ++c) refl_m[c] = make_double2(1.0, 0.0);
+  }
+  if (!refl64.p) {
+    LUM_TRY(refl64.alloc(sizeof(double2) * 6 * mtot));
+    LUM_TRY(refl32.alloc(sizeof(float2) * 6 * mtot));
+  }
+  double2* K = refl64.as<double2>();
+  fft_refl_table<<<grid_for(mtot), 256, 0, st>>>(M[0], M[1], M[2], gn[0], gn[1], gn[2], spacing,
+                                                 lo_z, z0, mode, k, S, K);
+  LUM_CHECK_LAUNCH();
+  LUM_TRY(fft_pass<double>(*this, K, 6, 2, false, M[0], M[1], nullptr, st));
+  LUM_TRY(fft_pass<double>(*this, K, 6, 1, false, M[0], M[2], nullptr, st));
+  LUM_TRY(fft_pass<double>(*this, K, 6, 0, false, M[1], M[2], nullptr, st));
+  narrow_spectra<<<grid_for(6 * mtot), 256, 0, st>>>(6 * mtot, K, refl32.as<float2>());
+  LUM_CHECK_LAUNCH();
+  return LUM_OK;
+}
+
 template <typename R>
 static lum_status fft_apply_t(FftOperator& op, typename Cx<R>::T* buf,
-                              const typename Cx<R>::T* kern, const double2* x, double2* y,
-                              cudaStream_t st, const int* skip) {
+                              const typename Cx<R>::T* kern, const typename Cx<R>::T* refl,
+                              const double2* x, double2* y, cudaStream_t st, const int* skip) {
   fft_scatter<R><<<grid_for(op.mtot), 256, 0, st>>>(op.mtot, op.d_node_dip.as<int>(), x, buf,
                                                     skip);
   LUM_CHECK_LAUNCH();
@@ -463,7 +606,19 @@ static lum_status fft_apply_t(FftOperator& op, typename Cx<R>::T* buf,
   LUM_TRY(fft_pass<R>(op, buf, 3, 2, false, op.gn[0], op.gn[1], skip, st));
   LUM_TRY(fft_pass<R>(op, buf, 3, 1, false, op.gn[0], op.M[2], skip, st));
   LUM_TRY(fft_pass<R>(op, buf, 3, 0, false, op.M[1], op.M[2], skip, st));
-  fft_spectral_product<R><<<grid_for(op.mtot), 256, 0, st>>>(op.mtot, kern, buf, skip);
+  if (refl) {
+    using T2 = typename Cx<R>::T;
+    T2 m[3];
+    for (int c = 0; c < 3; ++c) {
+      m[c].x = (R)op.refl_m[c].x;
+      m[c].y = (R)op.refl_m[c].y;
+    }
+    const int lines = op.M[0] * op.M[1];
+    fft_spectral_product_refl<R><<<grid_for((size_t)lines * (op.M[2] / 2 + 1)), 256, 0, st>>>(
+        lines, op.M[2], op.mtot, kern, refl, m[0], m[1], m[2], buf, skip);
+  } else {
+    fft_spectral_product<R><<<grid_for(op.mtot), 256, 0, st>>>(op.mtot, kern, buf, skip);
+  }
   LUM_CHECK_LAUNCH();
   // inverse: every x line, then only the lines that hold dipole nodes
   LUM_TRY(fft_pass<R>(op, buf, 3, 0, true, op.M[1], op.M[2], skip, st));
@@ -477,12 +632,20 @@ static lum_status fft_apply_t(FftOperator& op, typename Cx<R>::T* buf,
 
 lum_status FftOperator::apply(int precision, const double2* x, double2* y, cudaStream_t st,
                               cudaEvent_t ev0, cudaEvent_t ev1, const int* skip) {
+  if (refl_stale) {
+    set_error("the Sommerfeld spectra belong to another wavelength: call "
+              "lum_session_set_sommerfeld after lum_session_set_wavelength");
+    return LUM_ERR_INVALID;
+  }
   if (ev0) cudaEventRecord(ev0, st);
   lum_status s;
+  const bool r = refl_mode != 0;
   if (precision == LUM_FP32)
-    s = fft_apply_t<float>(*this, buf32.as<float2>(), kern32.as<float2>(), x, y, st, skip);
+    s = fft_apply_t<float>(*this, buf32.as<float2>(), kern32.as<float2>(),
+                           r ? refl32.as<float2>() : nullptr, x, y, st, skip);
   else
-    s = fft_apply_t<double>(*this, buf64.as<double2>(), kern64.as<double2>(), x, y, st, skip);
+    s = fft_apply_t<double>(*this, buf64.as<double2>(), kern64.as<double2>(),
+                            r ? refl64.as<double2>() : nullptr, x, y, st, skip);
   if (ev1) cudaEventRecord(ev1, st);
   return s;
 }

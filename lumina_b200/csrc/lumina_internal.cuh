@@ -268,6 +268,15 @@ struct FftOperator {
   DevBuf kern64, kern32;    // kernel spectra: 6 components (xx xy xz yy yz zz) x mtot
   DevBuf buf64, buf32;      // 3 vector components x mtot
   DevBuf tw64, tw32;        // twiddles exp(-2 pi i q / M[c]), q < M[c]/2, per axis
+  // Substrate term: R(da, db, c_i + c_j) is a convolution in the z-mirrored
+  // coordinate, applied as R^ . (m o X)(kx, ky, -kz) in the spectral product.
+  int refl_mode = 0;        // 0 none, 1 Fresnel image dipole, 2 Sommerfeld
+  int refl_stale = 0;       // Sommerfeld spectra of another wavelength
+  double lo_z = 0.0;        // lowest lattice node height (z of c = 0)
+  double2 refl_m[3] = {{1, 0}, {1, 0}, {1, 0}};  // column factors of the mirrored input
+  DevBuf refl64, refl32;    // reflected spectra: 6 components x mtot
+  lum_status set_reflection(int mode, const lum_substrate* fresnel, const SommDev* somm,
+                            cudaStream_t st);
   lum_status build(const double* pos_host, int n, double spacing, double cell, int use_fcd,
                    cudaStream_t st);
   lum_status set_physics(double k, const double* inv_alpha_host, cudaStream_t st);
@@ -361,6 +370,7 @@ const char* f32_variant_name(int v);    // otf.cu
 const char* f32x2_variant_name(int v);  // otf.cu
 lum_status somm_assemble(const OtfOperator& g, int precision, void* A, size_t ld,
                          cudaStream_t st);
+lum_status somm_params(const lum_sommerfeld* s, SommDev* out);
 lum_status assemble_from_table(const OtfOperator& g, int precision, void* A, size_t ld,
                                cudaStream_t st);  // table.cu
 

@@ -122,3 +122,69 @@ def test_fft_rejects_off_lattice_and_duplicates(backend, rng):
     with backend.create_fft_session(two, inv2, 0.012, True, 1.0, spacing=2.0) as S:
         assert rel_err(S.matvec(x, "fp64"),
                        orc.matvec_onthefly(two, alpha2, x, 0.012, True, 1.0)) < 1e-11
+
+
+# --- planar substrate through the z-mirrored convolution ---------------------
+from lumina_b200.lattice import SommerfeldRuntime, SubstrateRuntime  # noqa: E402
+
+SUB_CASES = ["fresnel_box", "fresnel_sphere", "sommerfeld_box", "sommerfeld_sphere",
+             "sommerfeld_layer"]
+
+
+def _sub_geometry(kind):
+    if kind.endswith("sphere"):
+        pos = discretise_primitive(Sphere((0.0, 0.0, 0.0), 6.0), 2.0).copy()
+        pos[:, 2] += 8.0
+        return pos, 2.0
+    if kind.endswith("layer"):
+        return _box(9, 6, 1, 2.0, origin=(-3.0, 1.0, 3.0)), 2.0
+    return _box(7, 5, 4, 1.5, origin=(-3.25, 1.5, 2.0)), 1.5
+
+
+@pytest.mark.parametrize("kind", SUB_CASES)
+def test_fft_substrate_matches_oracle(backend, rng, kind):
+    """The reflected term as a second convolution in the z-mirrored
+    coordinate equals the on-the-fly substrate term (assembly.rs:274-303)."""
+    pos, s = _sub_geometry(kind)
+    n = pos.shape[0]
+    alpha = _aniso_alpha(rng, n)
+    lam = 600.0
+    k = 2 * math.pi / lam
+    x = rand_vec(rng, 3 * n)
+    inv = lb.invert_polarisability(alpha)
+    if kind.startswith("fresnel"):
+        sub = SubstrateRuntime(0.5, 0.2 + 0.05j)
+        y_ref = orc.matvec_onthefly(pos, alpha, x, k, True, s, substrate=sub)
+    else:
+        sub = SommerfeldRuntime(0.5, lam, 2.25 + 0.1j, 1.0)
+        y_ref = orc.matvec_sommerfeld(pos, alpha, x, k, sub, True, s)
+    with backend.create_fft_session(pos, inv, k, True, s, substrate=sub) as S:
+        assert rel_err(S.matvec(x, "fp64"), y_ref) < 1e-12
+        assert rel_err(S.matvec(x, "fp32"), y_ref) < 2e-5
+
+
+def test_fft_sommerfeld_solve_and_wavelength_change(backend, rng):
+    pos = discretise_primitive(Sphere((0.0, 0.0, 0.0), 6.0), 2.0).copy()
+    pos[:, 2] += 9.0
+    w1 = configs.au_workload("s", pos, 2.0, 520.0)
+    w2 = configs.au_workload("s", pos, 2.0, 640.0)
+    s1 = SommerfeldRuntime(0.0, 520.0, 2.25, 1.0)
+    s2 = SommerfeldRuntime(0.0, 640.0, 2.2, 1.0)
+    inv1, inv2 = lb.invert_polarisability(w1.alpha), lb.invert_polarisability(w2.alpha)
+    A = orc.assemble_sommerfeld(w1.positions, w1.alpha, w1.k, s1, True, 2.0)
+    b = orc.incident_field(w1.positions, w1.k)
+    ref = orc.cross_sections(w1.positions, w1.alpha, orc.lu_solve(A, b), w1.k)
+    x2 = rand_vec(rng, 3 * w1.n)
+    with backend.create_fft_session(w1.positions, inv1, w1.k, True, 2.0, substrate=s1) as S:
+        x, info = S.solve(b, 1e-10, 5000, 30, "fp32_refine")
+        cs = lb.cross_sections(w1.positions, inv1, x, w1.k, lb.IncidentField())
+        assert info["converged"] and abs(cs[0] - ref[0]) / abs(ref[0]) < 1e-6
+        # the Fresnel-free re-target leaves the Sommerfeld spectra stale
+        S._lib.lum_session_set_wavelength(S._h, float(w2.k),
+                                          lb.backend._dp(np.ascontiguousarray(inv2).view(np.float64)),
+                                          None)
+        with pytest.raises(lb.SolverError):
+            S.matvec(x2, "fp64")
+        S.set_wavelength(w2.k, inv2, substrate=s2)
+        y = S.matvec(x2, "fp64")
+    assert rel_err(y, orc.matvec_sommerfeld(w2.positions, w2.alpha, x2, w2.k, s2, True, 2.0)) < 1e-12
