@@ -343,8 +343,10 @@ def main():
     # e2e through the public API with host arrays
     e2e = None
     if not args.no_e2e:
+        # the on-the-fly operator, as the device-timed value (the solver's FFT
+        # branch has its own line: --workload fft)
         solver = lb.CdaSolver(backend=bk, iterative_threshold=0, use_fcd=True, cell_size=1.0,
-                              matrix_memory_budget=0, precision="fp32_refine")
+                              matrix_memory_budget=0, precision="fp32_refine", use_fft=False)
         params = lb.SimulationParams(solver_tolerance=args.tol, max_iterations=args.max_iter)
         ds = [lb.DipoleSet(w.positions, w.alpha) for w in per]
         solver.compute_cross_sections(ds[0], lams[0], params)  # warm
@@ -1096,7 +1098,9 @@ def _bench_harmonic(args, bk, stream, torch, lb, configs):
             "scaling": "weak", "dtype": "f32+f64", "mode": "fp32_refine",
             "config": {"workload": "Au cuboid 60x50x10 nm (N=30,000), FCD 1 nm, fundamental "
                                    "800 nm, SHG at 400 nm, isotropic-surface chi(2), "
-                                   "GMRES(30) tol 1e-8", "n_dipoles": n},
+                                   "GMRES(30) tol 1e-8", "n_dipoles": n,
+                       "operator": "the solver's dispatch: the block-Toeplitz FFT session "
+                                   "for this lattice"},
             "iterations": info.get("iterations"), "converged": bool(info.get("converged")),
             "shg_intensity": r.intensity,
             "e2e": {"value": n / t, "unit": UNIT, "h2d_bytes_per_step": n * (24 + 144 + 48),

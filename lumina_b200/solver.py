@@ -12,6 +12,14 @@ cross sections) and the dispatch of :238-419 with every branch on the device:
   substrate terms included) + device GMRES on the cached matrix.
 * otherwise: the matrix-free on-the-fly session + device GMRES.
 
+Before the cached / on-the-fly branches, like the reference's FFT branch
+(:286-298), dipoles on a cubic lattice of pitch ``cell_size`` go through the
+block-Toeplitz FFT session.  The reference takes it only without FCD, lattice
+sum or substrate; the device FFT operator also carries FCD and both substrate
+forms, so here it is taken whenever there is no lattice sum and its
+estimated cost (6 M log2 M for an M-point circulant against N^2 pair
+evaluations) is lower.  ``use_fft=False`` turns the branch off.
+
 ``precision="fp64"`` runs plain FP64 GMRES; ``"fp32_refine"`` runs the FP32
 operator inside FP64 Arnoldi/Givens with FP64 restart residuals.
 """
@@ -41,6 +49,7 @@ class CdaSolver:
     precision: str = "fp64"
     direct_tolerance: float = 1e-12
     restart: int = 30
+    use_fft: bool = True
 
     def __post_init__(self):
         if self.backend is None:
@@ -57,10 +66,33 @@ class CdaSolver:
                          cell_size=cell_size, incident_field=incident_field, **kw)
 
     # ------------------------------------------------------------------
+    def _fft_worthwhile(self, positions: np.ndarray) -> bool:
+        """Lattice test of fft_matvec.rs:19-59 (pitch = cell_size, 1e-6
+        tolerance) and the cost estimate of the FFT branch."""
+        if not self.use_fft or self.lattice is not None or self.cell_size <= 0:
+            return False
+        p = np.asarray(positions, np.float64).reshape(-1, 3)
+        f = (p - p.min(axis=0)) / self.cell_size
+        r = np.rint(f)
+        if np.any(np.abs(f - r) >= 1e-6):
+            return False
+        gn = r.max(axis=0).astype(np.int64) + 1
+        if np.any(gn > 512):
+            return False
+        m = [1 << int(math.ceil(math.log2(max(2 * g - 1, 1)))) for g in gn]
+        mtot = float(m[0] * m[1] * m[2])
+        if len(np.unique(r.astype(np.int64) @ np.array([m[1] * m[2], m[2], 1]))) != p.shape[0]:
+            return False
+        return 6.0 * mtot * max(math.log2(mtot), 1.0) < float(p.shape[0]) ** 2
+
     def _session(self, dipoles: DipoleSet, inv_alpha, k, params, direct: bool):
         n = dipoles.n
         matrix_bytes = (3 * n) ** 2 * 16
         sub = params.substrate_runtime
+        if not direct and self._fft_worthwhile(dipoles.positions):
+            return self.backend.create_fft_session(dipoles.positions, inv_alpha, k,
+                                                   use_fcd=self.use_fcd,
+                                                   cell_size=self.cell_size, substrate=sub)
         if direct or matrix_bytes <= self.matrix_memory_budget:
             storage = "fp32" if (self.precision == "fp32_refine" and not direct) else "fp64"
             return self.backend.assemble_and_create_session(
