@@ -181,14 +181,16 @@ def test_cdasolver_dispatch_paths(backend):
 
 def test_cdasolver_fft_branch(backend):
     """The solver's FFT branch (cda/mod.rs:286-298, widened to FCD and the
-    substrate forms) agrees with the matrix-free branch."""
+    substrate forms) agrees with the matrix-free branch at the C_ext gate.
+    Tolerance 1e-8 as in the bench: FP32+refine through the FP32 FFT product
+    stalls near 1e-9 on this system."""
     from lumina_b200.lattice import SommerfeldRuntime
     w = configs.cuboid_au((20.0, 20.0, 10.0), 1.0, 520.0)
     pos = w.positions.copy()
     pos[:, 2] += 8.0
     ds = lb.DipoleSet(pos, w.alpha)
     for sub in (None, SommerfeldRuntime(0.0, 520.0, 2.25, 1.0)):
-        params = lb.SimulationParams(solver_tolerance=1e-10, max_iterations=5000,
+        params = lb.SimulationParams(solver_tolerance=1e-8, max_iterations=5000,
                                      substrate_runtime=sub)
         fft = lb.CdaSolver.with_fcd(0, True, 1.0, backend=backend, precision="fp32_refine")
         otf = lb.CdaSolver.with_fcd(0, True, 1.0, backend=backend, precision="fp32_refine",
@@ -196,7 +198,7 @@ def test_cdasolver_fft_branch(backend):
         assert fft._fft_worthwhile(pos) and not otf._fft_worthwhile(pos)
         a = fft.compute_cross_sections(ds, 520.0, params).extinction
         b = otf.compute_cross_sections(ds, 520.0, params).extinction
-        assert abs(a - b) / abs(b) < 1e-7
+        assert abs(a - b) / abs(b) < 1e-6
 
 
 # --- edge cases -----------------------------------------------------------
