@@ -327,6 +327,7 @@ struct BatchGeom {
   int K = 0, N = 0;
   int ell_w = 0;
   int lofree = 0, fast = 1;
+  int minb32 = 4;                      // FP32 pair kernel: CTAs per SM it is built for (4 or 6)
   int nparts32 = 1, nparts64 = 1;      // partial slices (max splits of any system)
   const int* sys_off = nullptr;        // [K+1]
   const int* row_sys = nullptr;        // [N]

@@ -1393,8 +1393,10 @@ __device__ __forceinline__ int batch_draw(unsigned* counters, int nitems, int* s
   return -1;
 }
 
-template <bool FAST, bool LOFREE>
-__global__ void __launch_bounds__(kOtfBlock, 6)
+// MINB 6: 80 registers, 24 warps per SM (some spill); MINB 4: no spills,
+// 16 warps per SM.
+template <bool FAST, bool LOFREE, int MINB>
+__global__ void __launch_bounds__(kOtfBlock, MINB)
 batch_pairs_f32(BatchGeom g, const double2* __restrict__ x, const int4* __restrict__ items,
                 int nitems, unsigned* counters, const BatchFlags* __restrict__ flags,
                 int skip_mode, float2* __restrict__ partial) {
@@ -1594,14 +1596,21 @@ lum_status batch_near_fcd(BatchGeom& g, int use_fcd, DevBuf& near_j, DevBuf& fcd
 int batch_occupancy(const BatchGeom& g, int precision) {
   int occ = 1;
   if (precision == LUM_FP32) {
+#define LUM_BATCH_OCC(F, L)                                                                  \
+  (g.minb32 == 4                                                                           \
+       ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_pairs_f32<F, L, 4>,      \
+                                                       kOtfBlock, 0)                       \
+       : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_pairs_f32<F, L, 6>,      \
+                                                       kOtfBlock, 0))
     if (g.fast && g.lofree)
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_pairs_f32<true, true>, kOtfBlock, 0);
+      LUM_BATCH_OCC(true, true);
     else if (g.fast)
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_pairs_f32<true, false>, kOtfBlock, 0);
+      LUM_BATCH_OCC(true, false);
     else if (g.lofree)
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_pairs_f32<false, true>, kOtfBlock, 0);
+      LUM_BATCH_OCC(false, true);
     else
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_pairs_f32<false, false>, kOtfBlock, 0);
+      LUM_BATCH_OCC(false, false);
+#undef LUM_BATCH_OCC
   } else {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_pairs_f64, kOtfBlock, 0);
   }
@@ -1661,9 +1670,15 @@ lum_status batch_apply(const BatchGeom& g, int precision, const double2* x, doub
   unsigned* cnt = q.counters.as<unsigned>();
   if (precision == LUM_FP32) {
     float2* part = static_cast<float2*>(partial);
-#define LUM_BATCH_F32(F, L)                                                             \
-  batch_pairs_f32<F, L><<<q.grid, kOtfBlock, 0, st>>>(g, x, items, q.nitems, cnt, flags, \
-                                                      skip_mode, part)
+#define LUM_BATCH_F32(F, L)                                                                 \
+  do {                                                                                       \
+    if (g.minb32 == 4)                                                                       \
+      batch_pairs_f32<F, L, 4><<<q.grid, kOtfBlock, 0, st>>>(g, x, items, q.nitems, cnt,     \
+                                                             flags, skip_mode, part);        \
+    else                                                                                     \
+      batch_pairs_f32<F, L, 6><<<q.grid, kOtfBlock, 0, st>>>(g, x, items, q.nitems, cnt,     \
+                                                             flags, skip_mode, part);        \
+  } while (0)
     if (g.fast && g.lofree)
       LUM_BATCH_F32(true, true);
     else if (g.fast)
