@@ -1033,7 +1033,7 @@ def _bench_sommerfeld(args, bk, stream, torch, lb, configs, fp32_peak):
                                              "d2h_bytes_per_step": rhs.nbytes}}
     pairs = float(n) * n
     achieved = pairs * SOMM_FLOPS_PER_PAIR / (apply_ms["fp32"] * 1e-3) / 1e12
-    line["roofline"] = {"bound": "fp32", "kernel": "somm_apply_rows<float> + free-space pairs",
+    line["roofline"] = {"bound": "fp32", "kernel": "somm_apply_keyed<float> + free-space pairs",
                         "achieved": achieved, "peak": fp32_peak / 1e3, "unit": "TFLOP/s",
                         "frac": achieved / (fp32_peak / 1e3),
                         "note": "lower bound: the whole FP32 application timed, only the "

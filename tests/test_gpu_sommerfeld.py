@@ -189,3 +189,38 @@ def test_invalid_sommerfeld_arguments(backend):
                                         substrate=SommerfeldRuntime(0.0, -1.0, 2.25, 1.0))
     with pytest.raises(lb.SolverError):
         backend.sommerfeld_tensor(SommerfeldRuntime(0.0, 600.0, 2.25, 0.0), pos[0], pos[1])
+
+
+@pytest.mark.parametrize("kind", ["onthefly", "cached", "fft"])
+def test_single_dipole_self_image(backend, rng, kind):
+    """N = 1: only the self block, G_refl(r, r) at rho = 0 (assembly.rs:157-166
+    runs for i == j), in each session kind."""
+    pos = np.array([[1.0, -2.0, 4.0]])
+    w = configs.au_workload("one", pos, 2.0, 600.0)
+    inv = lb.invert_polarisability(w.alpha)
+    somm = SommerfeldRuntime(0.0, 600.0, 2.25 + 0.3j, 1.0)
+    x = rng.standard_normal(3) + 1j * rng.standard_normal(3)
+    y_ref = orc.matvec_sommerfeld(pos, w.alpha, x, w.k, somm, True, 2.0)
+    if kind == "onthefly":
+        s = backend.create_onthefly_session(pos, inv, w.k, True, 2.0, substrate=somm)
+    elif kind == "cached":
+        s = backend.assemble_and_create_session(pos, w.k, inv, True, 2.0, substrate=somm,
+                                                precision="fp64")
+    else:
+        s = backend.create_fft_session(pos, inv, w.k, True, 2.0, substrate=somm)
+    with s:
+        assert rel_err(s.matvec(x, "fp64"), y_ref) < 1e-12
+
+
+def test_dipoles_below_interface_have_no_reflected_term(backend, rng):
+    """dz <= 0 gives a zero tensor (sommerfeld.rs:263-266): with the
+    interface above every dipole the operator is the free-space one."""
+    w, inv = _particle(wl=600.0)
+    somm = SommerfeldRuntime(float(w.positions[:, 2].max()) + 50.0, 600.0, 2.25, 1.0)
+    x = rng.standard_normal(3 * w.n) + 1j * rng.standard_normal(3 * w.n)
+    y_free = orc.matvec_onthefly(w.positions, w.alpha, x, w.k, True, 2.0)
+    for layout_jitter in (0.0, 1e-3):
+        pos = w.positions + rng.uniform(-layout_jitter, layout_jitter, w.positions.shape)
+        y_ref = orc.matvec_onthefly(pos, w.alpha, x, w.k, True, 2.0) if layout_jitter else y_free
+        with backend.create_onthefly_session(pos, inv, w.k, True, 2.0, substrate=somm) as s:
+            assert rel_err(s.matvec(x, "fp64"), y_ref) < 1e-12
