@@ -354,3 +354,36 @@ def test_ref_parallel_sessions(backend):
     for t in ts:
         t.join()
     assert all(e is not None and e < 1e-4 for e in errs)
+
+
+# --- the reference's benchmark-as-test (tests/gpu_benchmark.rs) ---------------
+def _bench_matrix(dim):
+    """gpu_benchmark.rs:16-30: a deterministic complex matrix made diagonally
+    dominant, and the vector of :33-41."""
+    i = np.arange(dim)[:, None]
+    j = np.arange(dim)[None, :]
+    A = (((i * 137 + j * 251 + 31) % 997) / 997.0 - 0.5) + \
+        1j * (((i * 173 + j * 311 + 59) % 991) / 991.0 - 0.5)
+    A[np.arange(dim), np.arange(dim)] += dim
+    q = np.arange(dim)
+    v = (((q * 193 + 41) % 983) / 983.0 - 0.5) + 1j * (((q * 229 + 67) % 977) / 977.0 - 0.5)
+    return A, v
+
+
+@pytest.mark.parametrize("dim", [300, 1000, 3000])
+def test_ref_benchmark_matvec_and_gmres(backend, dim):
+    """gpu_benchmark.rs:86-200: the FP32 session matvec agrees with the FP64
+    product to < 1e-4, and GMRES through it (tol 1e-6) with the FP64 GMRES at
+    1e-10 to < 1e-3 -- here the FP32+refine solve at 1e-10 is held to 1e-8."""
+    A, v = _bench_matrix(dim)
+    y_ref = A @ v
+    x_ref = np.linalg.solve(A, v)
+    with backend.create_session(dim, "fp32") as s:
+        s.upload_matrix(A)
+        assert rel_err(s.matvec(v, "fp32"), y_ref) < 1e-4
+        x, info = s.solve(v, 1e-6, 1000, 30, "fp64")
+        assert rel_err(x, x_ref) < 1e-3
+    with backend.create_session(dim, "fp64") as s:
+        s.upload_matrix(A)
+        x, info = s.solve(v, 1e-10, 1000, 30, "fp32_refine")
+        assert info["converged"] and rel_err(x, x_ref) < 1e-8
