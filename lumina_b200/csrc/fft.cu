@@ -417,7 +417,12 @@ static lum_status fft_pass(const FftOperator& op, typename Cx<R>::T* data, int n
     inner = sz;
   }
   const int cap = (sizeof(R) == 8) ? 1024 : 2048;  // B * L per CTA
-  const int B = std::max(1, std::min(n_inner, cap / L));
+  int B = std::max(1, std::min(n_inner, cap / L));
+  // fill the GPU: halve the lines per CTA while the grid has fewer than four
+  // CTAs per SM; strided lines keep at least 8 per CTA (coalesced loads)
+  const int bmin = (elem == 1) ? 1 : 8;
+  while (B > bmin && (long long)n_outer * ((n_inner + B - 1) / B) * ncomp < 4LL * 148)
+    B = std::max(bmin, B / 2);
   const size_t smem = sizeof(T2) * ((size_t)2 * B * (L + 1) + L / 2);
   const int chunks = (n_inner + B - 1) / B;
   const dim3 grid((unsigned)((size_t)n_outer * chunks), 1, ncomp);
