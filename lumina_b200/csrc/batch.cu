@@ -602,6 +602,11 @@ lum_status batch_workspace(lum_batch* B, int m) {
 lum_status rhs_apply(lum_batch* B, int prec, const double2* x, double2* y) {
   lum_session* s = B->src;
   const size_t n3 = (size_t)s->dim;
+  if (s->otf.has_somm && s->otf.somm_stale) {
+    set_error("the session's Sommerfeld term belongs to another wavelength: call "
+              "lum_session_set_sommerfeld after lum_session_set_wavelength");
+    return LUM_ERR_INVALID;
+  }
   if (s->kind == 1 && s->cached.precision == LUM_FP32 && prec == LUM_FP32)
     return s->cached.apply_multi(x, y, B->K, 1, (long long)n3, LUM_MATMUL_TENSOR, s->stream);
   if (s->kind == 1 && s->cached.precision == LUM_FP64)

@@ -634,6 +634,11 @@ static lum_status check_matmul(lum_session* s, const void* X, const void* Y, int
     set_error("invalid matmul method %d", method);
     return LUM_ERR_INVALID;
   }
+  if (s->otf.has_somm && s->otf.somm_stale) {
+    set_error("the matrix was not re-assembled for the new wavelength: call "
+              "lum_session_set_sommerfeld after lum_session_set_wavelength");
+    return LUM_ERR_INVALID;
+  }
   return LUM_OK;
 }
 

@@ -156,6 +156,9 @@ def test_set_wavelength_marks_table_stale_then_rebuilds(backend, rng):
                                               None)
             with pytest.raises(lb.SolverError):
                 s.matvec(x, "fp64")
+            if kind == "cached":  # nor may the multi-vector product use the old matrix
+                with pytest.raises(lb.SolverError):
+                    s.matmul(np.stack([x, x], axis=1), "cuda_cores")
             s.set_wavelength(w2.k, inv2, substrate=s2)
             assert rel_err(s.matvec(x, "fp64"), y_ref) < 1e-12
 
