@@ -141,7 +141,7 @@ def _harmonic_response(order, solver, omega_response: DipoleResponse, dipoles_h:
             x, info = sess.solve(rhs, params_h.solver_tolerance, params_h.max_iterations,
                                  solver.restart, solver.precision)
     finally:
-        sess.close()
+        solver._release(sess)
     driven = x.reshape(-1, 3)
     intensity = float(np.sum(np.abs(driven) ** 2))
     ff = None

@@ -20,12 +20,23 @@ forms, so here it is taken whenever there is no lattice sum and its
 estimated cost (6 M log2 M for an M-point circulant against N^2 pair
 evaluations) is lower.  ``use_fft=False`` turns the branch off.
 
+Successive calls on the same geometry and branch (a wavelength sweep, the
+runner's loop of runner.rs:150-183) re-target the solver's last session with
+``set_wavelength`` instead of building a new one: the geometry, near list,
+Krylov workspace and device buffers stay, and only k, alpha^-1 and the
+wavelength-dependent tables are rebuilt.  The kept session is released by
+``close()`` (or when the solver is collected); ``reuse_session=False`` builds
+one session per call.  A call that finds the kept session busy in another
+thread builds its own.
+
 ``precision="fp64"`` runs plain FP64 GMRES; ``"fp32_refine"`` runs the FP32
 operator inside FP64 Arnoldi/Givens with FP64 restart residuals.
 """
 from __future__ import annotations
 
+import hashlib
 import math
+import threading
 from dataclasses import dataclass, field
 from typing import Optional
 
@@ -50,10 +61,25 @@ class CdaSolver:
     direct_tolerance: float = 1e-12
     restart: int = 30
     use_fft: bool = True
+    reuse_session: bool = True
 
     def __post_init__(self):
         if self.backend is None:
             self.backend = be.CudaBackend(0)
+        self._kept = None            # (key, session) of the last call
+        self._kept_lock = threading.Lock()
+
+    def close(self) -> None:
+        """Release the session kept for re-use."""
+        kept, self._kept = getattr(self, "_kept", None), None
+        if kept is not None:
+            kept[1].close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
     @staticmethod
     def with_fcd(iterative_threshold, use_fcd, cell_size, **kw) -> "CdaSolver":
@@ -85,16 +111,34 @@ class CdaSolver:
             return False
         return 6.0 * mtot * max(math.log2(mtot), 1.0) < float(p.shape[0]) ** 2
 
-    def _session(self, dipoles: DipoleSet, inv_alpha, k, params, direct: bool):
+    def _plan(self, dipoles: DipoleSet, params, direct: bool):
+        """The branch of the dispatch, its storage, and the key under which a
+        session of it can be re-targeted to another wavelength."""
         n = dipoles.n
-        matrix_bytes = (3 * n) ** 2 * 16
         sub = params.substrate_runtime
+        storage = None
         if not direct and self._fft_worthwhile(dipoles.positions):
+            branch = "fft"
+        elif direct or (3 * n) ** 2 * 16 <= self.matrix_memory_budget:
+            branch = "cached"
+            storage = "fp32" if (self.precision == "fp32_refine" and not direct) else "fp64"
+        else:
+            branch = "onthefly"
+        pos = np.ascontiguousarray(np.asarray(dipoles.positions, np.float64))
+        geom = hashlib.blake2b(pos.tobytes(), digest_size=16).digest()
+        sub_kind = None if sub is None else ("sommerfeld" if hasattr(sub, "wavelength_nm")
+                                             else "fresnel")
+        key = (branch, storage, n, geom, bool(self.use_fcd), float(self.cell_size),
+               repr(self.lattice), tuple(float(v) for v in params.k_bloch), sub_kind)
+        return branch, storage, key
+
+    def _create(self, branch, storage, dipoles: DipoleSet, inv_alpha, k, params):
+        sub = params.substrate_runtime
+        if branch == "fft":
             return self.backend.create_fft_session(dipoles.positions, inv_alpha, k,
                                                    use_fcd=self.use_fcd,
                                                    cell_size=self.cell_size, substrate=sub)
-        if direct or matrix_bytes <= self.matrix_memory_budget:
-            storage = "fp32" if (self.precision == "fp32_refine" and not direct) else "fp64"
+        if branch == "cached":
             return self.backend.assemble_and_create_session(
                 dipoles.positions, k, inv_alpha, use_fcd=self.use_fcd, cell_size=self.cell_size,
                 lattice=self.lattice, k_bloch=params.k_bloch, substrate=sub, precision=storage)
@@ -102,8 +146,36 @@ class CdaSolver:
             dipoles.positions, inv_alpha, k, use_fcd=self.use_fcd, cell_size=self.cell_size,
             lattice=self.lattice, k_bloch=params.k_bloch, substrate=sub)
 
+    def _session(self, dipoles: DipoleSet, inv_alpha, k, params, direct: bool):
+        """A session for this call; hand it back with ``_release``."""
+        branch, storage, key = self._plan(dipoles, params, direct)
+        if not self.reuse_session or not self._kept_lock.acquire(blocking=False):
+            return self._create(branch, storage, dipoles, inv_alpha, k, params)
+        try:
+            if self._kept is not None and self._kept[0] == key:
+                sess = self._kept[1]
+                sess.set_wavelength(k, inv_alpha, substrate=params.substrate_runtime)
+                return sess
+            self.close()
+            sess = self._create(branch, storage, dipoles, inv_alpha, k, params)
+            self._kept = (key, sess)
+            return sess
+        except BaseException:
+            self.close()
+            self._kept_lock.release()
+            raise
+
+    def _release(self, sess) -> None:
+        if self._kept is not None and self._kept[1] is sess:
+            self._kept_lock.release()
+        else:
+            sess.close()
+
     def solve_dipoles(self, dipoles: DipoleSet, wavelength_nm: float,
                       params: SimulationParams) -> DipoleResponse:
+        return self._solve(dipoles, wavelength_nm, params)[0]
+
+    def _solve(self, dipoles: DipoleSet, wavelength_nm: float, params: SimulationParams):
         if dipoles.n == 0:
             raise be.InvalidGeometry("No dipoles provided")
         k = wavenumber(wavelength_nm, params.environment_n)
@@ -119,23 +191,24 @@ class CdaSolver:
                 x, info = sess.solve(rhs, params.solver_tolerance, params.max_iterations,
                                      self.restart, self.precision)
         finally:
-            sess.close()
+            self._release(sess)
         moments = x.reshape(-1, 3)
         local = np.einsum("nab,nb->na", inv_alpha, moments)  # E_loc = alpha^-1 p (:401-410)
-        return DipoleResponse(wavelength_nm, params.environment_n, moments, local, info)
+        return DipoleResponse(wavelength_nm, params.environment_n, moments, local, info), inv_alpha
 
     def cross_sections_from_response(self, dipoles: DipoleSet, response: DipoleResponse,
-                                     params: SimulationParams) -> CrossSections:
+                                     params: SimulationParams, _inv_alpha=None) -> CrossSections:
         k = wavenumber(response.wavelength_nm, params.environment_n)
-        inv_alpha = be.invert_polarisability(dipoles.polarisability)
+        inv_alpha = (be.invert_polarisability(dipoles.polarisability) if _inv_alpha is None
+                     else _inv_alpha)
         ext, ab, sca = be.cross_sections(dipoles.positions, inv_alpha, response.moments, k,
                                          self.incident_field)
         return CrossSections(response.wavelength_nm, ext, ab, sca)
 
     def compute_cross_sections(self, dipoles: DipoleSet, wavelength_nm: float,
                                params: SimulationParams) -> CrossSections:
-        resp = self.solve_dipoles(dipoles, wavelength_nm, params)
-        return self.cross_sections_from_response(dipoles, resp, params)
+        resp, inv_alpha = self._solve(dipoles, wavelength_nm, params)
+        return self.cross_sections_from_response(dipoles, resp, params, inv_alpha)
 
 
     def compute_near_field(self, dipoles: DipoleSet, response: DipoleResponse, plane):

@@ -387,3 +387,73 @@ def test_ref_benchmark_matvec_and_gmres(backend, dim):
         s.upload_matrix(A)
         x, info = s.solve(v, 1e-10, 1000, 30, "fp32_refine")
         assert info["converged"] and rel_err(x, x_ref) < 1e-8
+
+
+@pytest.mark.parametrize("branch", ["direct", "cached", "onthefly", "fft", "onthefly_sommerfeld"])
+def test_cdasolver_session_reuse_matches_fresh(backend, branch):
+    """A wavelength sweep through one solver re-targets its kept session; the
+    results equal those of a fresh session per call, and a new geometry gets
+    a new session."""
+    from lumina_b200.lattice import SommerfeldRuntime, SubstrateSpec, SubstrateRuntime
+    if branch == "fft":
+        w = configs.cuboid_au((20.0, 20.0, 10.0), 1.0, 520.0)
+        kw = dict(iterative_threshold=0, cell_size=1.0)
+    else:
+        w = configs.sphere_au_925()
+        kw = dict(iterative_threshold=1000 if branch == "direct" else 0, cell_size=2.0,
+                  matrix_memory_budget=0 if branch.startswith("onthefly") else 2 << 30)
+    pos = w.positions.copy()
+    pos[:, 2] += 20.0
+    reuse = lb.CdaSolver(backend=backend, **kw)
+    fresh = lb.CdaSolver(backend=backend, reuse_session=False, **kw)
+    spec = SubstrateSpec(0.0, "glass", True, branch.endswith("sommerfeld"))
+    kept = []
+    for wl in (520.0, 600.0, 700.0):
+        ds = lb.DipoleSet(pos, configs.au_workload("s", pos, kw["cell_size"], wl).alpha)
+        sub = SubstrateRuntime.from_spec(spec, 2.25, 1.0, wl) if "sommerfeld" in branch else None
+        params = lb.SimulationParams(solver_tolerance=1e-8, max_iterations=20000,
+                                     substrate_runtime=sub)
+        a = reuse.compute_cross_sections(ds, wl, params)
+        b = fresh.compute_cross_sections(ds, wl, params)
+        assert abs(a.extinction - b.extinction) <= 1e-9 * abs(b.extinction)
+        assert abs(a.absorption - b.absorption) <= 1e-9 * abs(b.absorption)
+        kept.append(reuse._kept[1])
+    assert kept[0] is kept[1] is kept[2]
+    moved = lb.DipoleSet(pos + 2.0 * kw["cell_size"], ds.polarisability)
+    reuse.compute_cross_sections(moved, 700.0, params)
+    assert reuse._kept[1] is not kept[0]
+    reuse.close()
+    assert reuse._kept is None
+
+
+def test_cdasolver_shared_between_threads(backend):
+    """Two threads on one solver: the kept session is never used by both at
+    once (a busy session makes the other call build its own)."""
+    w = configs.sphere_au_925()
+    solver = lb.CdaSolver(backend=backend, iterative_threshold=0, cell_size=2.0,
+                          matrix_memory_budget=0)
+    params = lb.SimulationParams(solver_tolerance=1e-10, max_iterations=20000)
+    wls = [520.0, 560.0, 600.0, 640.0]
+    ref = {wl: lb.CdaSolver(backend=backend, iterative_threshold=0, cell_size=2.0,
+                            matrix_memory_budget=0, reuse_session=False).compute_cross_sections(
+        lb.DipoleSet(w.positions, configs.au_workload("s", w.positions, 2.0, wl).alpha), wl,
+        params).extinction for wl in wls}
+    out, errs = {}, []
+
+    def run(ws):
+        try:
+            for wl in ws:
+                ds = lb.DipoleSet(w.positions, configs.au_workload("s", w.positions, 2.0, wl).alpha)
+                out[wl] = solver.compute_cross_sections(ds, wl, params).extinction
+        except Exception as e:  # noqa: BLE001
+            errs.append(e)
+
+    th = [threading.Thread(target=run, args=(wls[i::2],)) for i in range(2)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    assert not errs
+    for wl in wls:
+        assert abs(out[wl] - ref[wl]) <= 1e-8 * abs(ref[wl])
+    solver.close()
