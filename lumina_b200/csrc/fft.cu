@@ -27,9 +27,10 @@
 // further FFT.  The table holds R at height sums t = c + c' in [0, 2 n_z - 2]
 // and lateral displacements as for G.
 //
-// FFTs are hand-written: batched radix-2 Stockham passes (the autosort
-// formulation of Govindaraju et al., "High Performance Discrete Fourier
-// Transforms on Graphics Processors", SC 2008) along one axis at a time,
+// FFTs are hand-written: batched Stockham passes (the autosort formulation of
+// Govindaraju et al., "High Performance Discrete Fourier Transforms on
+// Graphics Processors", SC 2008; radix-4 stages, one radix-2 stage when
+// log2 L is odd) along one axis at a time,
 // each CTA transforming B lines in shared memory, all three vector
 // components in one launch.  Forward passes skip the lines that the zero
 // padding keeps empty; inverse passes skip the lines no dipole reads.
@@ -115,16 +116,60 @@ fft_lines(typename Cx<R>::T* __restrict__ data, size_t comp_stride, int L, int B
   __syncthreads();
   T2* a = s0;
   T2* c = s1;
-  for (int ns = 1; ns < L; ns <<= 1) {
-    const int step = half / ns;  // twiddle stride: exp(-2 pi i r / (2 ns)) = tw[r * L/(2 ns)]
+  // Stockham stages: one radix-2 stage when log2 L is odd, then radix-4
+  // stages (each one shared-memory round trip for two radix-2 levels).
+  int ns = 1;
+  if ((__ffs(L) - 1) & 1) {
     for (int q = threadIdx.x; q < nb * half; q += blockDim.x) {
       const int b = q / half, j = q % half;
-      const T2 v0 = a[b * LP + j];
+      const T2 v0 = a[b * LP + j], v1 = a[b * LP + j + half];
+      c[b * LP + 2 * j] = cadd(v0, v1);
+      c[b * LP + 2 * j + 1] = csub(v0, v1);
+    }
+    __syncthreads();
+    T2* t = a;
+    a = c;
+    c = t;
+    ns = 2;
+  }
+  const int quarter = L >> 2;
+  for (; ns < L; ns <<= 2) {
+    // x_m = a[j + m L/4] w^(m r), w = exp(-+2 pi i / (4 ns)), r = j mod ns;
+    // tw index of w^t is t L / (4 ns); indices >= L/2 use w(t + L/2) = -w(t)
+    const int step = quarter / ns;
+    for (int q = threadIdx.x; q < nb * quarter; q += blockDim.x) {
+      const int b = q / quarter, j = q % quarter;
       const int r = j & (ns - 1);
-      const T2 v1 = cmulT(a[b * LP + j + half], stw[r * step]);
-      const int d = ((j - r) << 1) + r;
-      c[b * LP + d] = cadd(v0, v1);
-      c[b * LP + d + ns] = csub(v0, v1);
+      const T2* ab = a + b * LP + j;
+      const T2 x0 = ab[0];
+      T2 x1 = ab[quarter], x2 = ab[2 * quarter], x3 = ab[3 * quarter];
+      if (r) {
+        const int t1 = r * step, t2 = 2 * t1, t3 = 3 * t1;
+        x1 = cmulT(x1, stw[t1]);
+        x2 = cmulT(x2, stw[t2]);
+        T2 w3 = stw[t3 < half ? t3 : t3 - half];
+        if (t3 >= half) {
+          w3.x = -w3.x;
+          w3.y = -w3.y;
+        }
+        x3 = cmulT(x3, w3);
+      }
+      // 4-point DFT with kernel exp(-+ i pi m q / 2): -i (forward) or +i (inverse)
+      const T2 s02 = cadd(x0, x2), d02 = csub(x0, x2);
+      const T2 s13 = cadd(x1, x3), d13 = csub(x1, x3);
+      T2 jd13;  // (-i) d13 forward, (+i) d13 inverse
+      if (INV) {
+        jd13.x = -d13.y;
+        jd13.y = d13.x;
+      } else {
+        jd13.x = d13.y;
+        jd13.y = -d13.x;
+      }
+      T2* cb = c + b * LP + ((j - r) << 2) + r;
+      cb[0] = cadd(s02, s13);
+      cb[ns] = cadd(d02, jd13);
+      cb[2 * ns] = csub(s02, s13);
+      cb[3 * ns] = csub(d02, jd13);
     }
     __syncthreads();
     T2* t = a;
