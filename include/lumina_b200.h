@@ -173,9 +173,14 @@ LUM_API int lum_session_create_onthefly(lum_ctx* ctx, int n_dipoles, const doubl
 LUM_API int lum_session_create_fft(lum_ctx* ctx, int n_dipoles, const double* pos,
                                    const double* inv_alpha, double k, int use_fcd,
                                    double cell_size, double spacing, lum_session** out);
-/* Re-targets an on-the-fly session to a new wavelength (k, alpha^-1,
- * substrate factor) keeping the geometry and near-pair list (the runner's
- * per-wavelength loop, runner.rs:150-183). */
+/* Re-targets a session to a new wavelength (k, alpha^-1, Fresnel substrate
+ * factor or NULL) keeping the geometry, near-pair list and buffers (the
+ * runner's per-wavelength loop, runner.rs:150-183): an on-the-fly session
+ * rebuilds its wavelength tables, an assembled session re-assembles its
+ * matrix, an FFT session rebuilds its kernel (and reflected) spectra.  A
+ * session with a Sommerfeld term keeps it stale -- its applications fail
+ * with INVALID -- until lum_session_set_sommerfeld gives this wavelength's
+ * substrate. */
 LUM_API int lum_session_set_wavelength(lum_session* s, double k, const double* inv_alpha,
                                const lum_substrate* substrate);
 /* The Sommerfeld substrate runtime in the sessions.  Replaces the
