@@ -426,7 +426,7 @@ void ewald_real(const Lattice& L, const double r[3], const double kb[3], double 
     double barg = kb[0] * lp[0] + kb[1] * lp[1] + kb[2] * lp[2];
     C phase = C{std::cos(barg), std::sin(barg)};
     double damp = L.is_2d ? erfc_as(eta * s_norm) : 1.0;
-    T3 gs;
+    T3 gs{};  // greens_at fills it: s_sq >= 1e-24 above
     greens_at(s, k, gs);
     for (int a = 0; a < 3; ++a)
       for (int b = 0; b < 3; ++b) g[a][b] = add(g[a][b], mul(muls(phase, damp), gs[a][b]));
