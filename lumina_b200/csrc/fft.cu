@@ -33,7 +33,10 @@
 // log2 L is odd) along one axis at a time,
 // each CTA transforming B lines in shared memory, all three vector
 // components in one launch.  Forward passes skip the lines that the zero
-// padding keeps empty; inverse passes skip the lines no dipole reads.
+// padding keeps empty and mask the padding of the lines they do transform
+// (it is never written); inverse passes skip the lines no dipole reads.  The
+// first forward pass reads x through the node map and the last inverse pass
+// writes y, so no scatter or gather kernel runs (except for single layers).
 // FP64 and FP32 variants: the FP32 product (FP32 FFTs against FP32 copies
 // of the FP64 kernel spectra) is the refinement inner operator, the FP64
 // one the residual operator.
@@ -76,12 +79,28 @@ template <typename T2> __device__ __forceinline__ T2 cmulT(T2 a, T2 b) {
 // is at + t * elem_stride; blockIdx.x covers n_outer x ceil(n_inner / B)
 // groups of B lines, blockIdx.z the vector component.  tw[q] =
 // exp(-2 pi i q / L), q < L/2 (conjugated for the inverse).
+// Line I/O of a pass.  mode 0 reads and writes the buffer; mode 1 (the first
+// forward pass) reads x through the node map instead of a scattered buffer;
+// mode 2 (the last inverse pass) writes y_i = alpha_i^-1 x_i - line / mtot at
+// the dipole nodes instead of the buffer.  Elements t >= valid of a line are
+// read as zero: the padding of the circulant is never written, only masked.
+struct FftIO {
+  int mode;
+  int valid;
+  const int* node_dip;       // [mtot] dipole on each node, -1 if none
+  const double2* x;          // [3n]
+  const double2* inv_alpha;  // [9][n]
+  double2* y;                // [3n]
+  int n;
+  double scale;              // 1 / mtot
+};
+
 template <typename R, bool INV>
 __global__ void __launch_bounds__(kFftThreads)
 fft_lines(typename Cx<R>::T* __restrict__ data, size_t comp_stride, int L, int B,
           long long elem_stride, int n_outer, long long outer_stride, int n_inner,
           long long inner_stride, const typename Cx<R>::T* __restrict__ tw,
-          const int* __restrict__ skip) {
+          const int* __restrict__ skip, FftIO io) {
   using T2 = typename Cx<R>::T;
   if (skip && *skip) return;
   extern __shared__ unsigned char fft_smem[];
@@ -94,8 +113,9 @@ fft_lines(typename Cx<R>::T* __restrict__ data, size_t comp_stride, int L, int B
   const int i0 = (blockIdx.x % chunks) * B;
   const int nb = min(B, n_inner - i0);
   if (outer >= n_outer) return;
-  T2* base = data + blockIdx.z * comp_stride + (size_t)outer * outer_stride +
-             (size_t)i0 * inner_stride;
+  const size_t line0 = (size_t)outer * outer_stride + (size_t)i0 * inner_stride;
+  const int comp = blockIdx.z;
+  T2* base = data + comp * comp_stride + line0;
   const int half = L >> 1;
   for (int q = threadIdx.x; q < half; q += blockDim.x) {
     T2 w = tw[q];
@@ -111,7 +131,23 @@ fft_lines(typename Cx<R>::T* __restrict__ data, size_t comp_stride, int L, int B
       b = q % nb;
       t = q / nb;
     }
-    s0[b * LP + t] = base[(size_t)b * inner_stride + (size_t)t * elem_stride];
+    const size_t off = (size_t)b * inner_stride + (size_t)t * elem_stride;
+    T2 v;
+    v.x = 0;
+    v.y = 0;
+    if (t < io.valid) {
+      if (io.mode == 1) {
+        const int i = io.node_dip[line0 + off];
+        if (i >= 0) {
+          const double2 xv = io.x[3 * (size_t)i + comp];
+          v.x = (R)xv.x;
+          v.y = (R)xv.y;
+        }
+      } else {
+        v = base[off];
+      }
+    }
+    s0[b * LP + t] = v;
   }
   __syncthreads();
   T2* a = s0;
@@ -185,7 +221,25 @@ fft_lines(typename Cx<R>::T* __restrict__ data, size_t comp_stride, int L, int B
       b = q % nb;
       t = q / nb;
     }
-    base[(size_t)b * inner_stride + (size_t)t * elem_stride] = a[b * LP + t];
+    const size_t off = (size_t)b * inner_stride + (size_t)t * elem_stride;
+    if (io.mode == 2) {
+      const int i = io.node_dip[line0 + off];
+      if (i >= 0) {
+        double sr = 0.0, si = 0.0;
+#pragma unroll
+        for (int e = 0; e < 3; ++e) {
+          const double2 m = io.inv_alpha[(size_t)(3 * comp + e) * io.n + i];
+          const double2 xe = io.x[3 * (size_t)i + e];
+          sr += m.x * xe.x - m.y * xe.y;
+          si += m.x * xe.y + m.y * xe.x;
+        }
+        const T2 v = a[b * LP + t];
+        io.y[3 * (size_t)i + comp] =
+            make_double2(sr - (double)v.x * io.scale, si - (double)v.y * io.scale);
+      }
+    } else {
+      base[off] = a[b * LP + t];
+    }
   }
 }
 
@@ -442,7 +496,8 @@ unsigned grid_for(size_t count) {
 template <typename R>
 static lum_status fft_pass(const FftOperator& op, typename Cx<R>::T* data, int ncomp, int ax,
                            bool inverse, int n_outer, int n_inner, const int* skip,
-                           cudaStream_t st) {
+                           cudaStream_t st, FftIO io = FftIO{0, -1, nullptr, nullptr, nullptr,
+                                                             nullptr, 0, 0.0}) {
   using T2 = typename Cx<R>::T;
   const int L = op.M[ax];
   if (L <= 1 || n_outer <= 0 || n_inner <= 0) return LUM_OK;
@@ -473,12 +528,13 @@ static lum_status fft_pass(const FftOperator& op, typename Cx<R>::T* data, int n
   const dim3 grid((unsigned)((size_t)n_outer * chunks), 1, ncomp);
   const T2* tw = reinterpret_cast<const T2*>(sizeof(R) == 8 ? op.tw64.p : op.tw32.p) +
                  op.tw_off[ax];
+  if (io.valid < 0) io.valid = L;
   if (inverse)
     fft_lines<R, true><<<grid, kFftThreads, smem, st>>>(data, op.mtot, L, B, elem, n_outer,
-                                                        outer, n_inner, inner, tw, skip);
+                                                        outer, n_inner, inner, tw, skip, io);
   else
     fft_lines<R, false><<<grid, kFftThreads, smem, st>>>(data, op.mtot, L, B, elem, n_outer,
-                                                         outer, n_inner, inner, tw, skip);
+                                                         outer, n_inner, inner, tw, skip, io);
   LUM_CHECK_LAUNCH();
   return LUM_OK;
 }
@@ -648,14 +704,29 @@ template <typename R>
 static lum_status fft_apply_t(FftOperator& op, typename Cx<R>::T* buf,
                               const typename Cx<R>::T* kern, const typename Cx<R>::T* refl,
                               const double2* x, double2* y, cudaStream_t st, const int* skip) {
-  fft_scatter<R><<<grid_for(op.mtot), 256, 0, st>>>(op.mtot, op.d_node_dip.as<int>(), x, buf,
-                                                    skip);
-  LUM_CHECK_LAUNCH();
+  // With more than one layer the first z pass reads x through the node map
+  // and the last one writes y (no scatter / gather kernels, no zero fill);
+  // a single layer (M_z = 1, no z pass) scatters and gathers.
+  const bool fused = op.M[2] > 1;
+  const FftIO plain{0, -1, nullptr, nullptr, nullptr, nullptr, 0, 0.0};
+  const FftIO load_x{1, op.gn[2], op.d_node_dip.as<int>(), x, nullptr, nullptr, op.n, 0.0};
+  const FftIO store_y{2, -1, op.d_node_dip.as<int>(), x, op.inv_alpha.as<double2>(), y, op.n,
+                      1.0 / (double)op.mtot};
+  if (!fused) {
+    fft_scatter<R><<<grid_for(op.mtot), 256, 0, st>>>(op.mtot, op.d_node_dip.as<int>(), x, buf,
+                                                      skip);
+    LUM_CHECK_LAUNCH();
+  }
   // forward: z lines of the occupied (x, y) box, y lines of the occupied x
-  // range, then every x line
-  LUM_TRY(fft_pass<R>(op, buf, 3, 2, false, op.gn[0], op.gn[1], skip, st));
-  LUM_TRY(fft_pass<R>(op, buf, 3, 1, false, op.gn[0], op.M[2], skip, st));
-  LUM_TRY(fft_pass<R>(op, buf, 3, 0, false, op.M[1], op.M[2], skip, st));
+  // range (y beyond the box masked), then every x line (x beyond it masked)
+  LUM_TRY(fft_pass<R>(op, buf, 3, 2, false, op.gn[0], op.gn[1], skip, st, load_x));
+  FftIO yv = plain, xv = plain;
+  if (fused) {
+    yv.valid = op.gn[1];
+    xv.valid = op.gn[0];
+  }
+  LUM_TRY(fft_pass<R>(op, buf, 3, 1, false, op.gn[0], op.M[2], skip, st, yv));
+  LUM_TRY(fft_pass<R>(op, buf, 3, 0, false, op.M[1], op.M[2], skip, st, xv));
   if (refl) {
     using T2 = typename Cx<R>::T;
     T2 m[3];
@@ -673,10 +744,14 @@ static lum_status fft_apply_t(FftOperator& op, typename Cx<R>::T* buf,
   // inverse: every x line, then only the lines that hold dipole nodes
   LUM_TRY(fft_pass<R>(op, buf, 3, 0, true, op.M[1], op.M[2], skip, st));
   LUM_TRY(fft_pass<R>(op, buf, 3, 1, true, op.gn[0], op.M[2], skip, st));
-  LUM_TRY(fft_pass<R>(op, buf, 3, 2, true, op.gn[0], op.gn[1], skip, st));
-  fft_gather<R><<<(op.n + 255) / 256, 256, 0, st>>>(op.n, op.mtot, op.d_grid_of.as<int>(),
-                                                    op.inv_alpha.as<double2>(), x, buf, y, skip);
-  LUM_CHECK_LAUNCH();
+  LUM_TRY(fft_pass<R>(op, buf, 3, 2, true, op.gn[0], op.gn[1], skip, st,
+                      fused ? store_y : plain));
+  if (!fused) {
+    fft_gather<R><<<(op.n + 255) / 256, 256, 0, st>>>(op.n, op.mtot, op.d_grid_of.as<int>(),
+                                                      op.inv_alpha.as<double2>(), x, buf, y,
+                                                      skip);
+    LUM_CHECK_LAUNCH();
+  }
   return LUM_OK;
 }
 
