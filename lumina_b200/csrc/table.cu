@@ -26,7 +26,11 @@
 namespace lum {
 
 constexpr int kTabBlock = 128;
-constexpr int kEntry = 10;  // complex slots per tensor (9 used)
+// The periodic tensor (like the point tensor) is symmetric, so an entry holds
+// its six distinct components xx xy xz yy yz zz: 48 B in FP32 (three 16-byte
+// loads), 96 B in FP64.  kSym[p][q] is the slot of component (p, q).
+constexpr int kEntry = 6;
+__device__ __constant__ int kSym[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
 
 __global__ void tab_build(int count, int Db, int Dc, int oa, int ob, int oc, double d,
                           int image, double zbase, LatticeDev L,
@@ -48,12 +52,31 @@ __global__ void tab_build(int count, int Db, int Dc, int oa, int ob, int oc, dou
   } else {
     ewald_tensor(L, lreal, lrecip, rx, ry, rz, kb, k, g);
   }
-  for (int q = 0; q < 9; ++q) {
-    t64[(size_t)e * kEntry + q] = g[q];
-    t32[(size_t)e * kEntry + q] = make_float2((float)g[q].x, (float)g[q].y);
+  const int upper[6] = {0, 1, 2, 4, 5, 8};
+  for (int q = 0; q < kEntry; ++q) {
+    const double2 v = g[upper[q]];
+    t64[(size_t)e * kEntry + q] = v;
+    t32[(size_t)e * kEntry + q] = make_float2((float)v.x, (float)v.y);
   }
-  t64[(size_t)e * kEntry + 9] = make_double2(0.0, 0.0);
-  t32[(size_t)e * kEntry + 9] = make_float2(0.f, 0.f);
+}
+
+// The six components of an entry in registers (FP32: three 16-byte loads).
+template <typename T2>
+__device__ __forceinline__ void tab_load(const T2* __restrict__ t, T2 c[6]);
+template <>
+__device__ __forceinline__ void tab_load<float2>(const float2* __restrict__ t, float2 c[6]) {
+  const float4* t4 = reinterpret_cast<const float4*>(t);
+#pragma unroll
+  for (int h = 0; h < 3; ++h) {
+    const float4 v = __ldg(t4 + h);
+    c[2 * h] = make_float2(v.x, v.y);
+    c[2 * h + 1] = make_float2(v.z, v.w);
+  }
+}
+template <>
+__device__ __forceinline__ void tab_load<double2>(const double2* __restrict__ t, double2 c[6]) {
+#pragma unroll
+  for (int h = 0; h < 6; ++h) c[h] = __ldg(t + h);
 }
 
 template <typename R> struct C2;
@@ -104,23 +127,25 @@ tab_pairs(int n, const int4* __restrict__ lidx, const double2* __restrict__ x,
     for (int jj = 0; jj < cnt; ++jj) {
       const int4 lj = sI[jj];
       const int ab = ((li.x - lj.x + oa) * Db + (li.y - lj.y + ob));
-      const T2* t = tab + ((size_t)ab * Dc + (li.z - lj.z + oc)) * kEntry;
+      T2 c[6];
+      tab_load<T2>(tab + ((size_t)ab * Dc + (li.z - lj.z + oc)) * kEntry, c);
+      constexpr int sym[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
 #pragma unroll
       for (int p = 0; p < 3; ++p)
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
-          const T2 g = __ldg(&t[3 * p + q]);
+          const T2 g = c[sym[p][q]];
           const T2 xv = sX[3 * jj + q];
           acc[2 * p] += g.x * xv.x - g.y * xv.y;
           acc[2 * p + 1] += g.x * xv.y + g.y * xv.x;
         }
       if (IMG) {
-        const T2* s = img + ((size_t)ab * Dcs + (li.z + lj.z)) * kEntry;
+        tab_load<T2>(img + ((size_t)ab * Dcs + (li.z + lj.z)) * kEntry, c);
 #pragma unroll
         for (int p = 0; p < 3; ++p)
 #pragma unroll
           for (int q = 0; q < 3; ++q) {
-            const T2 g = __ldg(&s[3 * p + q]);
+            const T2 g = c[sym[p][q]];
             const T2 xv = sM[3 * jj + q];
             acc[2 * p] += g.x * xv.x - g.y * xv.y;
             acc[2 * p + 1] += g.x * xv.y + g.y * xv.x;
@@ -270,11 +295,11 @@ assemble_table(int n, const int4* __restrict__ lidx, const double2* __restrict__
     for (int q = 0; q < 3; ++q) {
       double2 v = make_double2(0.0, 0.0);
       if (i == j) v = inv_alpha[(size_t)(3 * p + q) * n + i];
-      const double2 g = t[3 * p + q];
+      const double2 g = t[kSym[p][q]];
       v.x -= g.x;
       v.y -= g.y;
       if (s) {
-        const double2 h = s[3 * p + q];
+        const double2 h = s[kSym[p][q]];
         v.x -= m[q].x * h.x - m[q].y * h.y;
         v.y -= m[q].x * h.y + m[q].y * h.x;
       }
