@@ -6,7 +6,7 @@ dataset inside crates/lumina-materials/src/johnson_christy.rs (the
 writes them to ``johnson_christy_au.csv`` next to this file, so the package
 carries the data without reading the reference at run time.
 
-Usage: python extract_jc_table.py /path/to/reference
+Usage: python extract_jc_table.py <path of the Lumina source tree>
 """
 import os
 import re
@@ -31,4 +31,6 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        raise SystemExit(__doc__)
+    main(sys.argv[1])
