@@ -113,6 +113,11 @@ LUM_API int lum_device_info(lum_ctx* ctx, char* name, size_t name_len, size_t* m
                     int* compute_units);
 /* Message of the last failing call on this thread (never NULL). */
 LUM_API const char* lum_last_error(void);
+/* The sizes behind the last LUM_ERR_OOM on this thread, for
+ * ComputeError::OutOfMemory { requested, available } (backend.rs:13-22):
+ * the bytes the failed allocation asked for (0 when a CUDA call other than
+ * an allocation ran out) and the device's free bytes at that moment. */
+LUM_API int lum_last_oom(size_t* requested, size_t* available);
 /* Kernels this library has launched since load (all threads). */
 LUM_API uint64_t lum_launch_count(void);
 
@@ -221,7 +226,10 @@ LUM_API int lum_session_matvec(lum_session* s, int precision, const double* x, d
 LUM_API int lum_session_matvec_device(lum_session* s, int precision, const void* x_dev, void* y_dev,
                               void* stream);
 /* Multi-RHS cached matvec Y = A X, X and Y row-major dim x nrhs (device).
- * Method as LUM_MATMUL_AUTO below. */
+ * Method as LUM_MATMUL_AUTO below.  Asynchronous: a tensor-core pipeline
+ * wait that gave up is reported as TIMEOUT by the session's next
+ * synchronising product (lum_session_matmul_vectors, lum_batch_matvec,
+ * lum_batch_solve). */
 LUM_API int lum_session_matmul_device(lum_session* s, const void* X_dev, void* Y_dev, int nrhs,
                               void* stream);
 /* Methods of a multi-RHS cached product.  TENSOR runs on the tensor cores
@@ -277,7 +285,9 @@ LUM_API int lum_batch_matvec(lum_batch* b, int precision, const double* x, doubl
 LUM_API int lum_batch_matvec_device(lum_batch* b, int precision, const void* x_dev, void* y_dev);
 /* GMRES of lum_solve_gmres on every system at once; info has K entries.
  * Returns NOT_CONVERGED if any system did not converge (info says which),
- * DEVICE on a non-finite residual. */
+ * DEVICE on a non-finite residual, TIMEOUT if a tensor-core product of a
+ * right-hand-side batch gave up a pipeline wait (checked after every restart
+ * cycle; the solution is then not written). */
 LUM_API int lum_batch_solve(lum_batch* b, const double* rhs, double tol, int max_iter,
                             int restart, int mode, double* x, lum_solve_info* info);
 LUM_API int lum_batch_solve_device(lum_batch* b, const void* rhs_dev, void* x_dev, double tol,
@@ -400,6 +410,11 @@ LUM_API int lum_session_kernel_config(lum_session* s, char* buf, size_t len);
  * denominator for the compute-bound on-the-fly kernels: FP32 and FP64
  * GFLOP/s measured on the context's device. */
 LUM_API int lum_measure_fma_peak(lum_ctx* ctx, double* fp32_gflops, double* fp64_gflops);
+/* L2 read microbenchmark (16-byte loads that bypass L1 over a 16 MiB,
+ * L2-resident buffer), the roofline denominator for the table gathers of the
+ * periodic operator: GB/s on the context's device.  No counterpart in the
+ * reference. */
+LUM_API int lum_measure_l2_peak(lum_ctx* ctx, double* gbs);
 
 /* ---- allocation-free matvec ---------------------------------------------- */
 /* No counterpart in the reference.  For callers that cannot let a library
@@ -411,7 +426,8 @@ LUM_API int lum_measure_fma_peak(lum_ctx* ctx, double* fp32_gflops, double* fp64
  * (NULL = the legacy default stream) of the current device.  Its scratch is a
  * fixed 8 MiB device array inside the library; N above 174,762 is rejected
  * with LUM_ERR_INVALID.  The first call on each device looks up that array's
- * device address, so make it before any stream capture.  All calls share the
+ * device address, so make it before any stream capture; after a device reset
+ * (a new context) the next call looks it up again.  All calls share the
  * array: calls that overlap on the GPU race and must be serialised.  Nothing
  * is allocated or freed. */
 LUM_API int lum_matvec_onthefly_noalloc(int n_dipoles, const double* pos_dev,

@@ -7,7 +7,7 @@ input types (dipoles, materials, lattices, geometry).
 """
 from . import _ffi
 from .backend import (ComputeError, ConvergenceFailure, CudaBackend, CudaBatch, CudaSession,
-                      DeviceError,
+                      DeviceError, DeviceTimeout,
                       InvalidGeometry, OutOfMemory, SolverError, Unavailable, cross_sections,
                       incident_field, invert_polarisability)
 from .lattice import LatticeSpec, SommerfeldRuntime, SubstrateRuntime, SubstrateSpec
@@ -18,6 +18,7 @@ from .types import (CrossSections, Dipole, DipoleResponse, DipoleSet, IncidentFi
 
 __all__ = [
     "CudaBackend", "CudaSession", "CudaBatch", "CdaSolver", "ComputeError", "Unavailable", "DeviceError",
+    "DeviceTimeout",
     "OutOfMemory", "SolverError", "ConvergenceFailure", "InvalidGeometry", "LatticeSpec",
     "SubstrateSpec", "SubstrateRuntime", "SommerfeldRuntime", "Dipole", "DipoleSet", "IncidentField",
     "SimulationParams", "CrossSections", "DipoleResponse", "clausius_mossotti",

@@ -73,6 +73,7 @@ SIGNATURES = {
     "lum_ctx_destroy": (c_int, [c_void_p]),
     "lum_device_info": (c_int, [c_void_p, c_char_p, c_size_t, POINTER(c_size_t), POINTER(c_int)]),
     "lum_last_error": (c_char_p, []),
+    "lum_last_oom": (c_int, [POINTER(c_size_t), POINTER(c_size_t)]),
     "lum_launch_count": (c_uint64, []),
     "lum_invert_polarisability": (c_int, [c_int, _dp, _dp]),
     "lum_incident_field": (c_int, [c_int, _dp, _dp, _dp, c_double, c_double, _dp]),
@@ -113,6 +114,7 @@ SIGNATURES = {
                                   POINTER(c_int)]),
     "lum_session_kernel_config": (c_int, [c_void_p, c_char_p, c_size_t]),
     "lum_measure_fma_peak": (c_int, [c_void_p, POINTER(c_double), POINTER(c_double)]),
+    "lum_measure_l2_peak": (c_int, [c_void_p, POINTER(c_double)]),
     "lum_near_field": (c_int, [c_void_p, c_int, _dp, _dp, c_double, _dp, _dp, c_double, c_int,
                                _dp, c_void_p, c_void_p]),
     "lum_near_field_map": (c_int, [c_void_p, c_int, _dp, _dp, c_double, _dp, _dp, c_double,

@@ -33,8 +33,18 @@ class DeviceError(ComputeError):
     pass
 
 
+class DeviceTimeout(DeviceError):
+    """A bounded device-side wait gave up (LUM_ERR_TIMEOUT): the kernel
+    returned without finishing its result; the context stays usable."""
+
+
 class OutOfMemory(ComputeError):
-    pass
+    """ComputeError::OutOfMemory { requested, available } (backend.rs:13-22)."""
+
+    def __init__(self, msg: str, requested: int = 0, available: int = 0):
+        super().__init__(msg)
+        self.requested = requested
+        self.available = available
 
 
 class SolverError(Exception):
@@ -65,9 +75,13 @@ def _raise(rc: int, what: str = ""):
     if rc == _ffi.LUM_ERR_UNAVAILABLE:
         raise Unavailable(msg)
     if rc == _ffi.LUM_ERR_OOM:
-        raise OutOfMemory(msg)
+        req, avail = ctypes.c_size_t(0), ctypes.c_size_t(0)
+        _ffi.load().lum_last_oom(ctypes.byref(req), ctypes.byref(avail))
+        raise OutOfMemory(msg, req.value, avail.value)
     if rc == _ffi.LUM_ERR_INVALID:
         raise InvalidGeometry(msg)
+    if rc == _ffi.LUM_ERR_TIMEOUT:
+        raise DeviceTimeout(msg)
     raise DeviceError(msg)
 
 
@@ -667,6 +681,12 @@ class CudaBackend:
         f32, f64 = c_double(0.0), c_double(0.0)
         _raise(self._lib.lum_measure_fma_peak(self._h, byref(f32), byref(f64)), "fma peak")
         return f32.value, f64.value
+
+    def measure_l2_peak(self):
+        """L2 read bandwidth (GB/s) measured by a 16-byte-load kernel."""
+        g = c_double(0.0)
+        _raise(self._lib.lum_measure_l2_peak(self._h, byref(g)), "l2 peak")
+        return g.value
 
     def close(self):
         if getattr(self, "_h", None):

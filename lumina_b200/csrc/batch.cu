@@ -478,7 +478,8 @@ struct lum_batch {
   BatchGeom g;
   DevBuf d_off, d_row_sys, d_ns32, d_ns64, d_ch32, d_ch64, d_k, d_cell;
   DevBuf pos64, hi, lo, inv_alpha, near_j, fcd64, fcd32;
-  BatchQueue q32, q64;
+  BatchQueue q32, q64, qsym;
+  DevBuf d_nb;
   DevBuf part;
   DevBuf xin, yout;             // host-path staging of the matvec
   // solver workspace
@@ -564,6 +565,57 @@ struct RunResidual {
                           B->flags.as<BatchFlags>(), B->ctl.as<BatchCtl>());
   }
 };
+
+// Picks the FP32 pair scheme of a cluster batch (split work list or a
+// symmetric build) by timing; see the creation code for the override.
+lum_status batch_choose_scheme(lum_batch* B, cudaStream_t st) {
+  BatchGeom& g = B->g;
+  g.sym32 = 0;
+  const char* e = std::getenv("LUMINA_BATCH_SYM");
+  if (e && e[0] == '0') return LUM_OK;
+  if (e && e[0] >= '1' && e[0] <= '9') {
+    g.sym32 = std::min(e[0] - '0', batch_sym_variants());
+    return LUM_OK;
+  }
+  const size_t len = 3 * (size_t)B->N;
+  DevBuf xz, yz;
+  LUM_TRY(xz.alloc(sizeof(double2) * len));
+  LUM_TRY(yz.alloc(sizeof(double2) * len));
+  LUM_TRY_CUDA(cudaMemsetAsync(xz.p, 0, xz.bytes, st));
+  cudaEvent_t e0, e1;
+  LUM_TRY_CUDA(cudaEventCreate(&e0));
+  LUM_TRY_CUDA(cudaEventCreate(&e1));
+  float best = 1e30f;
+  int choice = 0;
+  lum_status status = LUM_OK;
+  for (int v = 0; v <= batch_sym_variants() && status == LUM_OK; ++v) {
+    g.sym32 = v;
+    float ms = 1e30f;
+    for (int rep = 0; rep < 4 && status == LUM_OK; ++rep) {
+      cudaEventRecord(e0, st);
+      status = batch_apply(g, LUM_FP32, xz.as<double2>(), yz.as<double2>(), B->part.p, B->q32,
+                           nullptr, 0, st);
+      cudaEventRecord(e1, st);
+      if (status != LUM_OK) break;
+      const cudaError_t ce = cudaEventSynchronize(e1);
+      if (ce != cudaSuccess) {
+        status = cuda_status(ce, "batch scheme timing", __FILE__, __LINE__);
+        break;
+      }
+      float t = 0.f;
+      cudaEventElapsedTime(&t, e0, e1);
+      if (rep > 0) ms = std::min(ms, t);  // the first launch warms
+    }
+    if (status == LUM_OK && ms < best) {
+      best = ms;
+      choice = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  g.sym32 = choice;
+  return status;
+}
 
 lum_status batch_workspace(lum_batch* B, int m) {
   const size_t len = 3 * (size_t)B->N;
@@ -853,9 +905,24 @@ int lum_batch_create(lum_ctx* ctx, int n_systems, const int* sys_dipoles, const 
   g.sys_chunk64 = B->d_ch64.as<int>();
   g.nparts32 = *std::max_element(ns32.begin(), ns32.end());
   g.nparts64 = *std::max_element(ns64.begin(), ns64.end());
-  const size_t pb = std::max(sizeof(float2) * (size_t)g.nparts32, sizeof(double2) * (size_t)g.nparts64) *
+  // The symmetric FP32 scheme (each unordered pair once, per-system
+  // superblock pairs): its work list, and the choice between it and the split
+  // kernel by timing one FP32 application of each (best of three after a warm
+  // launch).  LUMINA_BATCH_SYM=0 keeps the split kernel, =v forces build v.
+  std::vector<int> nb;
+  int sym_occ = 1;
+  for (int v = 1; v <= batch_sym_variants(); ++v) sym_occ = std::max(sym_occ, batch_sym_occupancy(g, v));
+  LUM_B_TRY(batch_queue_sym(off, sms * sym_occ, B->qsym, nb, st));
+  LUM_B_UP(B->d_nb, nb.data(), sizeof(int) * nb.size());
+  g.sys_nb = B->d_nb.as<int>();
+  g.qsym = &B->qsym;
+  const int nb_max = *std::max_element(nb.begin(), nb.end());
+  const size_t pb = std::max({sizeof(float2) * (size_t)g.nparts32,
+                              sizeof(double2) * (size_t)g.nparts64,
+                              sizeof(float2) * (size_t)nb_max}) *
                     3 * (size_t)N;
   LUM_B_TRY(B->part.alloc(pb));
+  LUM_B_TRY(batch_choose_scheme(B, st));
 #undef LUM_B_UP
 #undef LUM_B_TRY
   ce = cudaStreamSynchronize(st);
@@ -960,8 +1027,9 @@ int lum_batch_info(lum_batch* B, int* n_systems, int* n_dipoles, int* ell_width,
   if (ell_width) *ell_width = B->g.ell_w;
   if (cluster) *cluster = B->cl;
   if (elems_per_thread) *elems_per_thread = B->ept;
-  if (items32) *items32 = B->q32.nitems;
-  if (grid32) *grid32 = B->q32.grid;
+  const BatchQueue& q32 = B->g.sym32 ? B->qsym : B->q32;
+  if (items32) *items32 = q32.nitems;
+  if (grid32) *grid32 = q32.grid;
   if (items64) *items64 = B->q64.nitems;
   if (grid64) *grid64 = B->q64.grid;
   return LUM_OK;
@@ -994,6 +1062,7 @@ int lum_batch_matvec(lum_batch* B, int precision, const double* x, double* y) {
   LUM_TRY((lum_status)lum_batch_matvec_device(B, precision, B->xin.p, B->yout.p));
   LUM_TRY_CUDA(cudaMemcpyAsync(y, B->yout.p, bytes, cudaMemcpyDeviceToHost, B->stream));
   LUM_TRY_CUDA(cudaStreamSynchronize(B->stream));
+  if (B->src && B->src->kind == 1) return lum::cgemm_status(B->src->cached, B->stream);
   return LUM_OK;
 }
 
@@ -1034,9 +1103,14 @@ int lum_batch_solve_device(lum_batch* B, const void* b_dev, void* x_dev, double 
   LUM_TRY(dispatch_ept<RunInit>(B->ept, B, B->bs.as<const double2>()));
   // every active cycle advances each active system by >= 1 step
   const long max_cycles = (long)std::max(max_iter, 0) + 1;
+  // a tensor-core product whose pipeline wait gave up leaves tiles of its
+  // result unwritten: the cycle's status is read after every cycle
+  const bool tensor = B->src && B->src->kind == 1 && B->src->cached.precision == LUM_FP32 &&
+                      mode == LUM_SOLVE_FP32_REFINE;
   for (long cyc = 0; cyc < max_cycles; ++cyc) {
     LUM_TRY(batch_run_cycle(B, mode));
     LUM_TRY_CUDA(cudaStreamSynchronize(st));
+    if (tensor) LUM_TRY(lum::cgemm_status(B->src->cached, st));
     if (*B->h_active == 0) break;
   }
   LUM_TRY_CUDA(cudaMemcpyAsync(x_dev, B->xs.p, bytes, cudaMemcpyDeviceToDevice, st));

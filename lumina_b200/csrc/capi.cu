@@ -15,6 +15,7 @@ namespace lum {
 
 std::atomic<uint64_t> g_launches{0};
 static thread_local std::string t_last_error = "";
+static thread_local size_t t_oom_requested = 0, t_oom_available = 0;
 
 void set_error(const char* fmt, ...) {
   char buf[1024];
@@ -29,6 +30,10 @@ lum_status cuda_status(cudaError_t e, const char* what, const char* file, int li
   set_error("%s failed: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
   if (e == cudaErrorMemoryAllocation) {
     cudaGetLastError();  // clear the sticky-free allocation error
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    t_oom_requested = 0;
+    t_oom_available = fr;
     return LUM_ERR_OOM;
   }
   if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return LUM_ERR_UNAVAILABLE;
@@ -45,6 +50,8 @@ lum_status DevBuf::alloc(size_t nbytes) {
     cudaGetLastError();
     cudaMemGetInfo(&fr, &tot);
     set_error("Out of memory: requested %zu bytes, available %zu", nbytes, fr);
+    t_oom_requested = nbytes;
+    t_oom_available = fr;
     return LUM_ERR_OOM;
   }
   bytes = nbytes;
@@ -65,6 +72,24 @@ __global__ void fma_chain(T* out, int iters, T a, T b) {
   }
   T s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
   if (s == (T)-12345.678) out[0] = s;  // keeps the chain live; never true
+}
+
+// --- L2 read microbenchmark (roofline denominator for the table gathers) --
+// Every thread streams 16-byte loads that bypass L1 (ld.global.cg) over a
+// buffer far smaller than L2, so after the first pass every load hits L2.
+__global__ void l2_read(const float4* __restrict__ buf, size_t n4, int reps,
+                        float* __restrict__ out) {
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  const size_t t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  float acc = 0.f;
+  for (int r = 0; r < reps; ++r)
+    for (size_t i = (t0 + (size_t)r * 4099) % n4, c = 0; c < n4; c += stride) {
+      const float4 v = __ldcg(buf + i);
+      acc += v.x + v.y + v.z + v.w;
+      i += stride;
+      if (i >= n4) i -= n4;
+    }
+  if (acc == -12345.678f) out[0] = acc;  // keeps the loads live; never true
 }
 
 }  // namespace lum
@@ -147,6 +172,12 @@ static bool bad_ptr(const void* p, const char* what) {
 extern "C" {
 
 const char* lum_last_error(void) { return t_last_error.c_str(); }
+
+int lum_last_oom(size_t* requested, size_t* available) {
+  if (requested) *requested = t_oom_requested;
+  if (available) *available = t_oom_available;
+  return LUM_OK;
+}
 uint64_t lum_launch_count(void) { return g_launches.load(); }
 
 int lum_ctx_create(int device, lum_ctx** out) {
@@ -824,15 +855,52 @@ int lum_session_kernel_config(lum_session* s, char* buf, size_t len) {
   snprintf(buf, len,
            "kind=%s f32_variant=%s tuned_ms=%.4f nsplit32=%d nsplit64=%d ell_w=%d lofree=%d "
            "fast_trig=%d f32x2_variant=%s tuned_x2_ms=%.4f nsplit_x2=%d f32_sym=%d "
-           "tuned_sym_ms=%.4f sym_superblocks=%d sommerfeld=%s somm_records=%lld",
+           "sym_variant=%s tuned_sym_ms=%.4f f64_sym=%d tuned_f64_ms=%.4f f32x2_sym=%d "
+           "sym2_variant=%s sym_superblocks=%d sommerfeld=%s somm_records=%lld",
            s->kind == 0 ? "onthefly" : (s->kind == 1 ? "cached" : "fft"),
            lum::f32_variant_name(o.f32_variant),
            (double)o.tuned_ms, o.nsplit32, o.nsplit64, o.ell_w, o.lofree, o.fast_trig,
            lum::f32x2_variant_name(o.f32x2_variant), (double)o.tuned_x2_ms, o.nsplit_x2,
-           o.f32_sym, (double)o.tuned_sym_ms, o.sym_nb,
+           o.f32_sym, lum::sym_variant_name(o.f32_sym), (double)o.tuned_sym_ms, o.f64_sym,
+           (double)o.tuned_f64_ms, o.f32x2_sym, lum::sym2_variant_name(o.f32x2_sym), o.sym_nb,
            o.has_somm ? (o.somm_keyed ? "lattice_keys" : "pairs") : "none",
            (long long)o.somm_records);
   return LUM_OK;
+}
+
+int lum_measure_l2_peak(lum_ctx* ctx, double* gbs) {
+  if (bad_ptr(ctx, "ctx") || bad_ptr(gbs, "gbs")) return LUM_ERR_INVALID;
+  LUM_TRY_CUDA(cudaSetDevice(ctx->device));
+  const size_t bytes = size_t(16) << 20;  // 16 MiB: L2-resident
+  const size_t n4 = bytes / sizeof(float4);
+  DevBuf buf, out;
+  LUM_TRY(buf.alloc(bytes));
+  LUM_TRY(out.alloc(16));
+  LUM_TRY_CUDA(cudaMemset(buf.p, 0, bytes));
+  cudaEvent_t e0, e1;
+  LUM_TRY_CUDA(cudaEventCreate(&e0));
+  LUM_TRY_CUDA(cudaEventCreate(&e1));
+  const int threads = 512, blocks = ctx->sms * 4, reps = 64;
+  float ms = 0.f;
+  lum_status st = LUM_OK;
+  for (int rep = 0; rep < 2 && st == LUM_OK; ++rep) {  // the first launch warms L2
+    cudaEventRecord(e0);
+    l2_read<<<blocks, threads>>>(buf.as<float4>(), n4, reps, out.as<float>());
+    cudaEventRecord(e1);
+    const cudaError_t e = cudaEventSynchronize(e1);
+    if (e != cudaSuccess) st = cuda_status(e, "L2 microbenchmark", __FILE__, __LINE__);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+  }
+  if (st == LUM_OK) {
+    cudaEventElapsedTime(&ms, e0, e1);
+    // each thread reads ceil(n4 / threads in the grid) entries per pass
+    const size_t grid = (size_t)blocks * threads;
+    const double read = (double)grid * (double)((n4 + grid - 1) / grid) * sizeof(float4) * reps;
+    *gbs = read / (ms * 1e-3) / 1e9;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return st;
 }
 
 int lum_measure_fma_peak(lum_ctx* ctx, double* fp32_gflops, double* fp64_gflops) {

@@ -43,13 +43,22 @@
 // Every mbarrier wait is bounded by a clock64 deadline: on expiry the CTA
 // records a status code, stops issuing work, waits (bounded) for its copies
 // and MMAs in flight, releases TMEM and returns.  The host reports a
-// nonzero status as LUM_ERR_TIMEOUT.
+// nonzero status as LUM_ERR_TIMEOUT.  The pipeline waits use a limit passed
+// at launch (kWaitCycles, ~2 s, unless LUMINA_TC_WAIT_CYCLES sets another
+// positive count of SM clocks); the final waits for the copies and MMAs in
+// flight always use kWaitCycles, so a short pipeline limit never lets the
+// CTA release shared memory or TMEM under an operation that has not landed.
+// LUMINA_TC_WITHHOLD_SPLIT=1 makes the first CTA's split warps withhold their
+// arrival on the first stage, so that its MMA issuer's wait runs out: the
+// check that a wait which never completes ends with TIMEOUT and leaves the
+// context usable.
 #include "lumina_internal.cuh"
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <cstdlib>
 
 namespace lum {
 namespace {
@@ -108,13 +117,13 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
 }
 
 // Waits for the phase of `parity` to complete.  Gives up when `abort` is set
-// by another role or at the deadline (then sets *abort and the status).
+// by another role or after `limit` SM clocks (then sets *abort and the status).
 __device__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort, int* status,
-                          int code) {
+                          int code, long long limit) {
   const long long t0 = clock64();
   while (!mbar_try(bar, parity)) {
     if (abort && *abort) return false;
-    if (clock64() - t0 > kWaitCycles) {
+    if (clock64() - t0 > limit) {
       if (abort) *abort = 1;
       atomicCAS(status, 0, code);
       return false;
@@ -191,7 +200,8 @@ cgemm_tf32x3_kernel(const __grid_constant__ CUtensorMap map_a,
                     const __grid_constant__ CUtensorMap map_bhi,
                     const __grid_constant__ CUtensorMap map_blo, int dim, int ktiles,
                     int ktiles_per_split, int nrhs, double2* __restrict__ Y, long long syc,
-                    long long syr, float2* __restrict__ part, int* __restrict__ status) {
+                    long long syr, float2* __restrict__ part, int* __restrict__ status,
+                    long long wait_cycles, int withhold) {
   using C = TcCfg<NT>;
   constexpr int S = C::kStages;
   constexpr int CPT = NT / 2;  // accumulator columns per epilogue thread
@@ -250,7 +260,7 @@ cgemm_tf32x3_kernel(const __grid_constant__ CUtensorMap map_a,
       const int s = it % S;
       const uint32_t ph = (it / S) & 1;
       if (*abort) break;
-      if (it >= S && !mbar_wait(&empty[s], ph ^ 1u, abort, status, 1)) break;
+      if (it >= S && !mbar_wait(&empty[s], ph ^ 1u, abort, status, 1, wait_cycles)) break;
       mbar_expect_tx(&full[s], kATileBytes + 2 * C::kBTileBytes);
       const int kx = (kt0 + it) * kTcBK;
       tma_load_2d(sA + s * kATileBytes, &map_a, kx, m0, &full[s]);
@@ -259,7 +269,7 @@ cgemm_tf32x3_kernel(const __grid_constant__ CUtensorMap map_a,
     }
     // copies still in flight must land before the CTA's shared memory is released
     for (int q = max(0, it - S); q < it; ++q)
-      mbar_wait(&full[q % S], (q / S) & 1, nullptr, status, 2);
+      mbar_wait(&full[q % S], (q / S) & 1, nullptr, status, 2, kWaitCycles);
   } else if (warp == 1 && lane == 0) {
     // ---- MMA issuer.  Chain c (kChain stages) accumulates into TMEM buffer
     // c & 1; the epilogue warps drain it while chain c + 1 runs.
@@ -271,9 +281,9 @@ cgemm_tf32x3_kernel(const __grid_constant__ CUtensorMap map_a,
       const bool first = (it % kChain) == 0;
       const uint32_t acc = tmem + (uint32_t)((c & 1) * NT);
       if (first && c >= 2 &&
-          !mbar_wait(&acc_empty[c & 1], ((c >> 1) - 1) & 1, abort, status, 6))
+          !mbar_wait(&acc_empty[c & 1], ((c >> 1) - 1) & 1, abort, status, 6, wait_cycles))
         break;
-      if (!mbar_wait(&split[s], ph, abort, status, 3)) break;
+      if (!mbar_wait(&split[s], ph, abort, status, 3, wait_cycles)) break;
       tc_fence_after();
       const uint32_t a = smem_u32(sA + s * kATileBytes);
       const uint32_t alo = smem_u32(sAlo + s * kATileBytes);
@@ -292,7 +302,7 @@ cgemm_tf32x3_kernel(const __grid_constant__ CUtensorMap map_a,
     }
     // no MMA may be in flight when TMEM is released (also after an abort)
     mma_commit(done);
-    mbar_wait(done, 0, nullptr, status, 7);
+    mbar_wait(done, 0, nullptr, status, 7, kWaitCycles);
   } else if (warp >= 4) {
     // ---- split A into TF32 hi / lo; drain finished chains into registers;
     // write the result.  Warp 4 + 4h + q owns TMEM lanes 32q.. (rows) and
@@ -305,7 +315,7 @@ cgemm_tf32x3_kernel(const __grid_constant__ CUtensorMap map_a,
     for (int e = 0; e < CPT; ++e) sum[e] = 0.f;
     bool ok = true;
     auto drain = [&](int c) {
-      if (!mbar_wait(&acc_full[c & 1], (c >> 1) & 1, abort, status, 5)) {
+      if (!mbar_wait(&acc_full[c & 1], (c >> 1) & 1, abort, status, 5, wait_cycles)) {
         ok = false;
         return;
       }
@@ -324,7 +334,7 @@ cgemm_tf32x3_kernel(const __grid_constant__ CUtensorMap map_a,
     for (int it = 0; it < nk && ok; ++it) {
       const int s = it % S;
       const uint32_t ph = (it / S) & 1;
-      if (!mbar_wait(&full[s], ph, abort, status, 4)) {
+      if (!mbar_wait(&full[s], ph, abort, status, 4, wait_cycles)) {
         ok = false;
         break;
       }
@@ -346,7 +356,8 @@ cgemm_tf32x3_kernel(const __grid_constant__ CUtensorMap map_a,
       }
       // make these generic-proxy writes visible to the tensor core (async proxy)
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      mbar_arrive(&split[s]);
+      if (!(withhold && it == 0 && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0))
+        mbar_arrive(&split[s]);
       // the chain before the one this stage starts is complete: drain it
       if (it % kChain == 0 && it > 0) drain(it / kChain - 1);
     }
@@ -472,8 +483,16 @@ lum_status launch_tc(CachedOperator& op, int nrhs, int mt, int nt, int ksplit, i
   const CUtensorMap* mh = reinterpret_cast<const CUtensorMap*>(w.map_bhi);
   const CUtensorMap* ml = reinterpret_cast<const CUtensorMap*>(w.map_blo);
   float2* part = ksplit > 1 ? w.part.as<float2>() : nullptr;
+  long long wait_cycles = kWaitCycles;
+  if (const char* env = std::getenv("LUMINA_TC_WAIT_CYCLES")) {
+    const long long v = std::atoll(env);
+    if (v > 0) wait_cycles = v;
+  }
+  const char* wh = std::getenv("LUMINA_TC_WITHHOLD_SPLIT");
+  const int withhold = (wh && wh[0] == '1') ? 1 : 0;
   cgemm_tf32x3_kernel<NT><<<dim3(mt, nt, ksplit), kTcThreads, C::kSmemBytes, st>>>(
-      *ma, *mh, *ml, op.dim, ktiles, kps, nrhs, Y, syc, syr, part, w.status.as<int>());
+      *ma, *mh, *ml, op.dim, ktiles, kps, nrhs, Y, syc, syr, part, w.status.as<int>(),
+      wait_cycles, withhold);
   LUM_CHECK_LAUNCH();
   return LUM_OK;
 }

@@ -130,14 +130,22 @@ struct OtfOperator {
   float tuned_ms = 0.f;     // tuned FP32 pair-kernel time (ms), 0 if untuned
   // Symmetric scheme (pairs_f32_sym.cuh): each unordered pair evaluated once
   // over superblock pairs; chosen by the tuner when it is faster.
-  int f32_sym = 0;          // 0: split kernel; 2 or 3: symmetric kernel, CTAs per SM
+  int f32_sym = 0;          // 0: split kernel; v >= 1: symmetric build v (sym_variant_name)
+  int f64_sym = 0;          // 1: the FP64 operator runs the symmetric scheme too
+  int f32x2_sym = 0;        // two-vector FP32 applications: v >= 1 symmetric build v
   int sym_nb = 0, sym_nitems = 0;
   float tuned_sym_ms = 0.f;
+  float tuned_f64_ms = 0.f;
   DevBuf sym_items;         // int2 [sym_nitems] superblock pairs (I <= J)
-  DevBuf sym_slots;         // float2 [sym_nb][3n] per-superblock partial sums
+  DevBuf sym_slots;         // [sym_nb][3n] per-superblock partial sums (double2; float2 for FP32)
+  DevBuf sym_slots2;        // the second vector's FP64 slots (two-vector applications)
   lum_status sym_prepare(cudaStream_t st);
-  void sym_launch(int minb, const double2* x, const int* skip, cudaStream_t st);
+  void sym_launch(int variant, const double2* x, const int* skip, cudaStream_t st);
+  void sym64_launch(const double2* x, const int* skip, cudaStream_t st);
+  void sym2_launch(int variant, const double2* x, const double2* x2, const int* skip,
+                   const int* skip2, cudaStream_t st);
   lum_status tune_f32(cudaStream_t st);
+  lum_status tune_f64(cudaStream_t st);
   std::vector<double> host_pos;  // double4 host copy (image positions are built from it)
 
   // Sommerfeld substrate (sommerfeld.cu): the reflected-tensor integrals
@@ -328,6 +336,9 @@ struct BatchGeom {
   int ell_w = 0;
   int lofree = 0, fast = 1;
   int minb32 = 4;                      // FP32 pair kernel: CTAs per SM it is built for (4 or 6)
+  int sym32 = 0;                       // FP32: v >= 1 runs symmetric build v (batch_sym_name)
+  const int* sys_nb = nullptr;         // [K] superblocks of each system (symmetric scheme)
+  const struct BatchQueue* qsym = nullptr;  // symmetric work list
   int nparts32 = 1, nparts64 = 1;      // partial slices (max splits of any system)
   const int* sys_off = nullptr;        // [K+1]
   const int* row_sys = nullptr;        // [N]
@@ -366,9 +377,20 @@ lum_status batch_apply(const BatchGeom& g, int precision, const double2* x, doub
                        void* partial, BatchQueue& q, const BatchFlags* flags, int skip_mode,
                        cudaStream_t st);                                             // otf.cu
 int batch_occupancy(const BatchGeom& g, int precision);                              // otf.cu
+lum_status batch_queue_sym(const std::vector<int>& off, int slots, BatchQueue& q,
+                           std::vector<int>& nb, cudaStream_t st);                   // otf.cu
+int batch_sym_variants();                                                            // otf.cu
+const char* batch_sym_name(int v);                                                   // otf.cu
+int batch_sym_occupancy(const BatchGeom& g, int v);                                  // otf.cu
 
 const char* f32_variant_name(int v);    // otf.cu
 const char* f32x2_variant_name(int v);  // otf.cu
+const char* sym_variant_name(int v);    // otf.cu (1-based; "none" for 0)
+const char* sym2_variant_name(int v);   // otf.cu (1-based; "none" for 0)
+// Persistent tuner choices (tune_cache.cu).
+std::string tune_device_tag();
+bool tune_lookup(const std::string& key, int* value);
+void tune_store(const std::string& key, int value);
 lum_status somm_assemble(const OtfOperator& g, int precision, void* A, size_t ld,
                          cudaStream_t st);
 lum_status somm_params(const lum_sommerfeld* s, SommDev* out);

@@ -131,7 +131,28 @@ noalloc_epilogue(int n, const double2* __restrict__ x, const double2* __restrict
 namespace {
 constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mu;
+// Per device: the resolved address and the context it belongs to.  A device
+// reset (cudaDeviceReset) or a new primary context reloads this library's
+// device code, and the array may then sit at another address, so the address
+// is looked up again whenever the current context is not the recorded one.
 double2* g_noalloc_ptr[kMaxDevices] = {};
+void* g_noalloc_ctx[kMaxDevices] = {};
+
+using CtxGetCurrentFn = int (*)(void**);  // CUresult cuCtxGetCurrent(CUcontext*)
+
+CtxGetCurrentFn ctx_get_current() {
+  static CtxGetCurrentFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<CtxGetCurrentFn>(p);
+  }
+  return fn;
+}
 }  // namespace
 
 }  // namespace lum
@@ -164,10 +185,13 @@ extern "C" int lum_matvec_onthefly_noalloc(int n_dipoles, const double* pos,
   }
   double2* scratch = nullptr;
   {
-    // First call on a device: resolve the device address of the file-scope
-    // array (the host-side symbol is only a stand-in) with that device current.
+    // First call on a device (or in a new context of it): resolve the device
+    // address of the file-scope array (the host-side symbol is only a
+    // stand-in) with that device current.
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
+    void* ctx = nullptr;
+    if (CtxGetCurrentFn get = ctx_get_current()) get(&ctx);
+    if (!g_noalloc_ptr[dev] || ctx != g_noalloc_ctx[dev]) {
       void* p = nullptr;
       cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
       if (e != cudaSuccess || !p) {
@@ -175,6 +199,8 @@ extern "C" int lum_matvec_onthefly_noalloc(int n_dipoles, const double* pos,
                            "cudaGetSymbolAddress(no-alloc scratch)", __FILE__, __LINE__);
       }
       g_noalloc_ptr[dev] = static_cast<double2*>(p);
+      if (!ctx && ctx_get_current()) ctx_get_current()(&ctx);  // created by the lookup
+      g_noalloc_ctx[dev] = ctx;
     }
     scratch = g_noalloc_ptr[dev];
   }

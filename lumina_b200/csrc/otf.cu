@@ -41,6 +41,7 @@ constexpr int kOtfBlock = 128;
 }  // namespace lum
 #include "pairs_f32x2.cuh"
 #include "pairs_f32_sym.cuh"
+#include "pairs_f64_sym.cuh"
 namespace lum {
 
 // ---------------------------------------------------------------------------
@@ -655,7 +656,6 @@ const F32X2VariantEntry kF32X2Variants[] = {
     {"x2_rows4_minb3", 4, F32X2Variant<2, 3>::launch<false>, F32X2Variant<2, 3>::launch<true>, F32X2Variant<2, 3>::occupancy},
 };
 constexpr int kNumF32X2Variants = sizeof(kF32X2Variants) / sizeof(kF32X2Variants[0]);
-std::map<std::tuple<int, int, int>, int> g_tune_x2_cache;
 
 }  // namespace
 
@@ -926,6 +926,7 @@ lum_status OtfOperator::set_physics(double k_, const double* inv_alpha_host, int
                                   sizeof(double2) * (size_t)nsplit64 * 2) * 3 * (size_t)n;
     LUM_TRY(partial.alloc(bytes));
   }
+  if (first) LUM_TRY(tune_f64(st));
   if (first || old_fast != fast_trig) {
     LUM_TRY(tune_f32(st));
     f32x2_variant = -1;  // the two-vector variant is tuned again on first use
@@ -933,13 +934,58 @@ lum_status OtfOperator::set_physics(double k_, const double* inv_alpha_host, int
   return LUM_OK;
 }
 
-// Autotuner of the FP32 pair kernel: every variant (rows per thread x
-// register cap, with its own wave-filling split) is timed on this geometry
-// and the fastest is kept.  Choices are cached for the process per
-// (N, trig flavour, lo-free); LUMINA_TUNE=0 keeps the first variant.
+// Autotuner of the pair kernels: every build of the FP32 kernel (split
+// variants: rows per thread x register cap, each with its own wave-filling
+// split; symmetric variants) and both FP64 schemes are timed on this
+// geometry -- one warm launch, then the best of three -- and the fastest is
+// kept.  Choices are cached in memory and in the tuner's JSON file
+// (tune_cache.cu) per (device, kernel build, N, trig flavour, flags);
+// LUMINA_TUNE=0 keeps the first split variant and the split FP64 kernel.
 namespace {
-std::mutex g_tune_mu;
-std::map<std::tuple<int, int, int>, int> g_tune_cache;
+const char kKernelBuild[] = __DATE__ "_" __TIME__;
+
+std::string tune_key(const char* family, int n, int trig, int flags) {
+  std::string build(kKernelBuild);
+  for (char& c : build)
+    if (c == ' ') c = '_';
+  return std::string(family) + "|" + tune_device_tag() + "|" + build + "|n=" +
+         std::to_string(n) + "|trig=" + std::to_string(trig) + "|flags=" + std::to_string(flags);
+}
+
+// One warm launch, then the best of three timed launches.
+template <typename F>
+lum_status time_best(F&& launch, cudaStream_t st, cudaEvent_t e0, cudaEvent_t e1,
+                     const char* what, float* best_ms) {
+  launch();
+  float best = 1e30f;
+  for (int rep = 0; rep < 3; ++rep) {
+    cudaEventRecord(e0, st);
+    launch();
+    cudaEventRecord(e1, st);
+    cudaError_t e = cudaEventSynchronize(e1);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_status(e, what, __FILE__, __LINE__);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    best = std::min(best, ms);
+  }
+  g_launches.fetch_add(4, std::memory_order_relaxed);
+  *best_ms = best;
+  return LUM_OK;
+}
+
+struct EventPair {
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  ~EventPair() {
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+  }
+  lum_status create() {
+    LUM_TRY_CUDA(cudaEventCreate(&e0));
+    LUM_TRY_CUDA(cudaEventCreate(&e1));
+    return LUM_OK;
+  }
+};
 }  // namespace
 
 // Superblock pairs (I <= J) and the per-superblock partial sums of the
@@ -954,19 +1000,21 @@ lum_status OtfOperator::sym_prepare(cudaStream_t st) {
   LUM_TRY(sym_items.alloc(sizeof(int2) * items.size()));
   LUM_TRY_CUDA(cudaMemcpyAsync(sym_items.p, items.data(), sizeof(int2) * items.size(),
                                cudaMemcpyHostToDevice, st));
-  LUM_TRY(sym_slots.alloc(sizeof(float2) * (size_t)nb * 3 * (size_t)n));
+  // sized for the FP64 scheme; the FP32 scheme uses the first half (or both
+  // halves for two vectors)
+  LUM_TRY(sym_slots.alloc(sizeof(double2) * (size_t)nb * 3 * (size_t)n));
   LUM_TRY_CUDA(cudaStreamSynchronize(st));  // items is freed on return
   sym_nb = nb;
   sym_nitems = (int)items.size();
   return LUM_OK;
 }
 
-template <int MINB>
+template <int MINB, int RP>
 static void sym_launch_t(const OtfOperator& o, const double2* x, const int* skip,
                          cudaStream_t st) {
   const float kf = (float)o.k, s0f = (float)(o.k * o.k * o.k / (4.0 * kPi));
 #define LUM_SYM_LAUNCH(F, L)                                                                  \
-  otf_pairs_f32_sym<F, L, MINB><<<o.sym_nitems, kSymThreads, 0, st>>>(                        \
+  otf_pairs_f32_sym<F, L, MINB, RP><<<o.sym_nitems, SymShape<RP>::kThreads, 0, st>>>(         \
       o.n, o.pos_hi.as<float4>(), o.pos_lo.as<float4>(), x, kf, s0f, o.sym_items.as<int2>(), \
       o.sym_slots.as<float2>(), skip)
   if (o.fast_trig && o.lofree)
@@ -980,52 +1028,110 @@ static void sym_launch_t(const OtfOperator& o, const double2* x, const int* skip
 #undef LUM_SYM_LAUNCH
 }
 
-void OtfOperator::sym_launch(int minb, const double2* x, const int* skip, cudaStream_t st) {
-  if (minb >= 3)
-    sym_launch_t<3>(*this, x, skip, st);
+template <int MINB, int RP>
+static void sym2_launch_t(const OtfOperator& o, const double2* x, const double2* x2,
+                          const int* skip, const int* skip2, cudaStream_t st) {
+  const float kf = (float)o.k, s0f = (float)(o.k * o.k * o.k / (4.0 * kPi));
+  float2* s1 = o.sym_slots.as<float2>();
+  float2* s2 = s1 + (size_t)o.sym_nb * 3 * (size_t)o.n;
+#define LUM_SYM2_LAUNCH(F, L)                                                                 \
+  otf_pairs_f32_sym2<F, L, MINB, RP><<<o.sym_nitems, SymShape<RP>::kThreads, 0, st>>>(        \
+      o.n, o.pos_hi.as<float4>(), o.pos_lo.as<float4>(), x, x2, kf, s0f,                     \
+      o.sym_items.as<int2>(), s1, s2, skip, skip2)
+  if (o.fast_trig && o.lofree)
+    LUM_SYM2_LAUNCH(true, true);
+  else if (o.fast_trig)
+    LUM_SYM2_LAUNCH(true, false);
+  else if (o.lofree)
+    LUM_SYM2_LAUNCH(false, true);
   else
-    sym_launch_t<2>(*this, x, skip, st);
+    LUM_SYM2_LAUNCH(false, false);
+#undef LUM_SYM2_LAUNCH
+}
+
+namespace {
+// Builds of the symmetric FP32 scheme the tuner chooses from: rows per
+// thread (2 or 4) x CTAs per SM (the register cap).  f32_sym is 1 + the
+// index into this table, 0 for the split kernels.
+struct SymVariantEntry {
+  const char* name;
+  void (*launch)(const OtfOperator&, const double2*, const int*, cudaStream_t);
+};
+const SymVariantEntry kSymVariants[] = {
+    {"sym_rows2_minb2", sym_launch_t<2, 1>},
+    {"sym_rows2_minb3", sym_launch_t<3, 1>},
+    {"sym_rows4_minb4", sym_launch_t<4, 2>},
+    {"sym_rows4_minb3", sym_launch_t<3, 2>},
+};
+constexpr int kNumSymVariants = sizeof(kSymVariants) / sizeof(kSymVariants[0]);
+
+// Two-vector builds of the symmetric scheme; f32x2_sym is 1 + the index.
+struct Sym2VariantEntry {
+  const char* name;
+  void (*launch)(const OtfOperator&, const double2*, const double2*, const int*, const int*,
+                 cudaStream_t);
+};
+const Sym2VariantEntry kSym2Variants[] = {
+    {"sym2_rows2_minb2", sym2_launch_t<2, 1>},
+    {"sym2_rows2_minb1", sym2_launch_t<1, 1>},
+    {"sym2_rows4_minb2", sym2_launch_t<2, 2>},
+};
+constexpr int kNumSym2Variants = sizeof(kSym2Variants) / sizeof(kSym2Variants[0]);
+}  // namespace
+
+const char* sym_variant_name(int v) {
+  return (v >= 1 && v <= kNumSymVariants) ? kSymVariants[v - 1].name : "none";
+}
+
+const char* sym2_variant_name(int v) {
+  return (v >= 1 && v <= kNumSym2Variants) ? kSym2Variants[v - 1].name : "none";
+}
+
+void OtfOperator::sym_launch(int variant, const double2* x, const int* skip, cudaStream_t st) {
+  kSymVariants[std::min(std::max(variant, 1), kNumSymVariants) - 1].launch(*this, x, skip, st);
+}
+
+void OtfOperator::sym2_launch(int variant, const double2* x, const double2* x2, const int* skip,
+                              const int* skip2, cudaStream_t st) {
+  kSym2Variants[std::min(std::max(variant, 1), kNumSym2Variants) - 1].launch(*this, x, x2, skip,
+                                                                            skip2, st);
+}
+
+void OtfOperator::sym64_launch(const double2* x, const int* skip, cudaStream_t st) {
+  otf_pairs_f64_sym<<<sym_nitems, kSym64Threads, 0, st>>>(
+      n, pos64.as<double4>(), x, k, 1.0 / k, k * k * k / (4.0 * kPi), sym_items.as<int2>(),
+      sym_slots.as<double2>(), skip);
 }
 
 lum_status OtfOperator::tune_f32(cudaStream_t st) {
   f32_variant = 0;
   f32_sym = 0;
-  // LUMINA_F32_SYM=2 or 3 forces the symmetric scheme with 2 or 3 CTAs per SM
-  // (isolated systems; 1 means 2), =0
-  // excludes it; unset, the tuner decides by timing.
+  nsplit32 = nsplit_v[0];
+  const bool isolated = !has_lattice && !has_substrate;
+  // LUMINA_F32_SYM=v (1..4) forces symmetric build v on isolated systems
+  // (no lattice, no substrate image); =0 excludes the symmetric scheme.
   const char* sym_env = std::getenv("LUMINA_F32_SYM");
-  if (sym_env && (sym_env[0] == '2' || sym_env[0] == '3' || sym_env[0] == '1') &&
-      !has_lattice && !has_substrate) {
-    nsplit32 = nsplit_v[0];
-    f32_sym = sym_env[0] == '3' ? 3 : 2;
+  if (isolated && sym_env && sym_env[0] >= '1' && sym_env[0] <= '9') {
+    f32_sym = std::min(sym_env[0] - '0', kNumSymVariants);
     return sym_prepare(st);
   }
-  const bool sym_allowed = !(sym_env && sym_env[0] == '0');
+  const bool sym_allowed = isolated && !(sym_env && sym_env[0] == '0');
   const char* env = std::getenv("LUMINA_TUNE");
-  if ((env && env[0] == '0') || n < 2048) {
-    nsplit32 = nsplit_v[0];
-    return LUM_OK;
+  if ((env && env[0] == '0') || n < 2048) return LUM_OK;
+  const std::string key = tune_key("f32", n, fast_trig,
+                                   lofree + 2 * (isolated ? 0 : 1) + 4 * (sym_allowed ? 0 : 1));
+  int choice = 0;
+  if (tune_lookup(key, &choice)) {
+    f32_variant = std::min(std::max(choice % 100, 0), kNumF32Variants - 1);
+    f32_sym = sym_allowed ? std::min(choice / 100, kNumSymVariants) : 0;
+    nsplit32 = nsplit_v[f32_variant];
+    return f32_sym ? sym_prepare(st) : LUM_OK;
   }
-  const auto key = std::make_tuple(n, fast_trig, lofree + 2 * (has_lattice || has_substrate) +
-                                                     4 * (sym_allowed ? 0 : 1));
-  bool known = false;
-  {
-    std::lock_guard<std::mutex> lk(g_tune_mu);
-    auto it = g_tune_cache.find(key);
-    if (it != g_tune_cache.end()) {
-      f32_variant = it->second % 100;
-      f32_sym = (!has_lattice && !has_substrate) ? it->second / 100 : 0;
-      nsplit32 = nsplit_v[f32_variant];
-      known = true;
-    }
-  }
-  if (known) return f32_sym ? sym_prepare(st) : LUM_OK;
   DevBuf xz;
   LUM_TRY(xz.alloc(sizeof(double2) * 3 * (size_t)n));
   LUM_TRY_CUDA(cudaMemsetAsync(xz.p, 0, xz.bytes, st));
-  cudaEvent_t e0, e1;
-  LUM_TRY_CUDA(cudaEventCreate(&e0));
-  LUM_TRY_CUDA(cudaEventCreate(&e1));
+  EventPair ev;
+  LUM_TRY(ev.create());
   const int ntiles = (n + kOtfBlock - 1) / kOtfBlock;
   const double s0 = k * k * k / (4.0 * kPi);
   float best = 1e30f;
@@ -1038,59 +1144,78 @@ lum_status OtfOperator::tune_f32(cudaStream_t st) {
               make_float2(1.f, 0.f), make_float2(1.f, 0.f), (float)k, (float)(1.0 / k),
               (float)s0, chunk, partial.as<float2>(), nullptr};
     float ms = 0.f;
-    for (int rep = 0; rep < 2; ++rep) {  // first launch warms, second is timed
-      cudaEventRecord(e0, st);
-      kF32Variants[v].direct(fast_trig, lofree, grid, st, a);
-      cudaEventRecord(e1, st);
-    }
-    cudaError_t e = cudaEventSynchronize(e1);
-    if (e == cudaSuccess) e = cudaGetLastError();
-    if (e != cudaSuccess) {
-      cudaEventDestroy(e0);
-      cudaEventDestroy(e1);
-      return cuda_status(e, "pair-kernel tuning", __FILE__, __LINE__);
-    }
-    g_launches.fetch_add(2, std::memory_order_relaxed);
-    cudaEventElapsedTime(&ms, e0, e1);
+    LUM_TRY(time_best([&] { kF32Variants[v].direct(fast_trig, lofree, grid, st, a); }, st,
+                      ev.e0, ev.e1, "pair-kernel tuning", &ms));
     if (ms < best) {
       best = ms;
       f32_variant = v;
     }
   }
   // the symmetric scheme (isolated systems: no lattice, no substrate image)
-  f32_sym = 0;
-  if (!has_lattice && !has_substrate && sym_allowed) {
+  if (sym_allowed) {
     LUM_TRY(sym_prepare(st));
     tuned_sym_ms = 1e30f;
-    for (int minb = 2; minb <= 3; ++minb) {
+    for (int v = 1; v <= kNumSymVariants; ++v) {
       float ms = 0.f;
-      for (int rep = 0; rep < 2; ++rep) {
-        cudaEventRecord(e0, st);
-        sym_launch(minb, xz.as<double2>(), nullptr, st);
-        cudaEventRecord(e1, st);
-      }
-      cudaError_t e = cudaEventSynchronize(e1);
-      if (e == cudaSuccess) e = cudaGetLastError();
-      if (e != cudaSuccess) {
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
-        return cuda_status(e, "symmetric pair-kernel tuning", __FILE__, __LINE__);
-      }
-      g_launches.fetch_add(2, std::memory_order_relaxed);
-      cudaEventElapsedTime(&ms, e0, e1);
+      LUM_TRY(time_best([&] { sym_launch(v, xz.as<double2>(), nullptr, st); }, st, ev.e0,
+                        ev.e1, "symmetric pair-kernel tuning", &ms));
       tuned_sym_ms = std::min(tuned_sym_ms, ms);
       if (ms < best) {
         best = ms;
-        f32_sym = minb;
+        f32_sym = v;
       }
     }
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   nsplit32 = nsplit_v[f32_variant];
   tuned_ms = best;
-  std::lock_guard<std::mutex> lk(g_tune_mu);
-  g_tune_cache[key] = f32_variant + 100 * f32_sym;  // f32_sym: 0, 2 or 3
+  tune_store(key, f32_variant + 100 * f32_sym);
+  return LUM_OK;
+}
+
+// FP64 scheme: the split kernel (otf_pairs_f64) or, on isolated systems, the
+// symmetric one (otf_pairs_f64_sym); LUMINA_F64_SYM=1 forces the symmetric
+// scheme there, =0 excludes it.
+lum_status OtfOperator::tune_f64(cudaStream_t st) {
+  f64_sym = 0;
+  const bool isolated = !has_lattice && !has_substrate;
+  if (!isolated) return LUM_OK;
+  const char* sym_env = std::getenv("LUMINA_F64_SYM");
+  if (sym_env && sym_env[0] == '0') return LUM_OK;
+  if (sym_env && sym_env[0] == '1') {
+    f64_sym = 1;
+    return sym_prepare(st);
+  }
+  const char* env = std::getenv("LUMINA_TUNE");
+  if ((env && env[0] == '0') || n < 2048) return LUM_OK;
+  const std::string key = tune_key("f64", n, 0, 0);
+  int choice = 0;
+  if (tune_lookup(key, &choice)) {
+    f64_sym = choice ? 1 : 0;
+    return f64_sym ? sym_prepare(st) : LUM_OK;
+  }
+  LUM_TRY(sym_prepare(st));
+  DevBuf xz;
+  LUM_TRY(xz.alloc(sizeof(double2) * 3 * (size_t)n));
+  LUM_TRY_CUDA(cudaMemsetAsync(xz.p, 0, xz.bytes, st));
+  EventPair ev;
+  LUM_TRY(ev.create());
+  const int ntiles = (n + kOtfBlock - 1) / kOtfBlock;
+  const int ns = nsplit64;
+  const int chunk = ((ntiles + ns - 1) / ns) * kOtfBlock;
+  const double2 one = make_double2(1.0, 0.0);
+  float ms_split = 0.f, ms_sym = 0.f;
+  LUM_TRY(time_best(
+      [&] {
+        otf_pairs_f64<false><<<dim3(ntiles, ns), kOtfBlock, 0, st>>>(
+            n, pos64.as<double4>(), xz.as<double2>(), one, one, one, 0.0, k, 1.0 / k,
+            k * k * k / (4.0 * kPi), chunk, partial.as<double2>(), nullptr);
+      },
+      st, ev.e0, ev.e1, "FP64 pair-kernel tuning", &ms_split));
+  LUM_TRY(time_best([&] { sym64_launch(xz.as<double2>(), nullptr, st); }, st, ev.e0, ev.e1,
+                    "FP64 symmetric pair-kernel tuning", &ms_sym));
+  tuned_f64_ms = std::min(ms_split, ms_sym);
+  f64_sym = ms_sym < ms_split ? 1 : 0;
+  tune_store(key, f64_sym);
   return LUM_OK;
 }
 
@@ -1182,6 +1307,17 @@ lum_status OtfOperator::apply(int precision, const double2* x, double2* y, cudaS
     return LUM_OK;
   }
   // FP64
+  if (f64_sym && !has_substrate) {
+    if (ev0) cudaEventRecord(ev0, st);
+    sym64_launch(x, skip, st);
+    LUM_CHECK_LAUNCH();
+    if (ev1) cudaEventRecord(ev1, st);
+    otf_epilogue<double2, double2><<<epi_blocks, 256, 0, st>>>(
+        n, x, inv_alpha.as<double2>(), sym_slots.as<double2>(), sym_nb, ell_w,
+        near_j.as<int>(), fcd64.as<double2>(), y, skip);
+    LUM_CHECK_LAUNCH();
+    return LUM_OK;
+  }
   const int ns = nsplit64;
   const int chunk = ((ntiles + ns - 1) / ns) * kOtfBlock;
   dim3 grid(ntiles, ns);
@@ -1225,27 +1361,33 @@ lum_status OtfOperator::tune_f32_x2(cudaStream_t st) {
                                           sms));
   }
   f32x2_variant = 0;
-  const char* env = std::getenv("LUMINA_TUNE");
-  const auto key = std::make_tuple(n, fast_trig, lofree);
-  if ((env && env[0] == '0') || n < 2048) {
-    nsplit_x2 = ns_v[0];
-    return LUM_OK;
+  f32x2_sym = 0;
+  nsplit_x2 = ns_v[0];
+  const bool isolated = !has_lattice && !has_substrate;
+  // LUMINA_F32_SYM=v forces symmetric build v here too (the two-vector build
+  // of that number, capped at the last), =0 excludes the symmetric scheme
+  const char* sym_env = std::getenv("LUMINA_F32_SYM");
+  if (isolated && sym_env && sym_env[0] >= '1' && sym_env[0] <= '9') {
+    f32x2_sym = std::min(sym_env[0] - '0', kNumSym2Variants);
+    return sym_prepare(st);
   }
-  {
-    std::lock_guard<std::mutex> lk(g_tune_mu);
-    auto it = g_tune_x2_cache.find(key);
-    if (it != g_tune_x2_cache.end()) {
-      f32x2_variant = it->second;
-      nsplit_x2 = ns_v[f32x2_variant];
-      return LUM_OK;
-    }
+  const bool sym_allowed = isolated && !(sym_env && sym_env[0] == '0');
+  const char* env = std::getenv("LUMINA_TUNE");
+  if ((env && env[0] == '0') || n < 2048) return LUM_OK;
+  const std::string key = tune_key("f32x2", n, fast_trig,
+                                   lofree + 2 * (isolated ? 0 : 1) + 4 * (sym_allowed ? 0 : 1));
+  int choice = 0;
+  if (tune_lookup(key, &choice)) {
+    f32x2_variant = std::min(std::max(choice % 100, 0), kNumF32X2Variants - 1);
+    f32x2_sym = sym_allowed ? std::min(choice / 100, kNumSym2Variants) : 0;
+    nsplit_x2 = ns_v[f32x2_variant];
+    return f32x2_sym ? sym_prepare(st) : LUM_OK;
   }
   DevBuf xz;
   LUM_TRY(xz.alloc(sizeof(double2) * 3 * (size_t)n));
   LUM_TRY_CUDA(cudaMemsetAsync(xz.p, 0, xz.bytes, st));
-  cudaEvent_t e0, e1;
-  LUM_TRY_CUDA(cudaEventCreate(&e0));
-  LUM_TRY_CUDA(cudaEventCreate(&e1));
+  EventPair ev;
+  LUM_TRY(ev.create());
   const double s0 = k * k * k / (4.0 * kPi);
   float best = 1e30f;
   for (int v = 0; v < kNumF32X2Variants; ++v) {
@@ -1258,31 +1400,29 @@ lum_status OtfOperator::tune_f32_x2(cudaStream_t st) {
                 (float)k, (float)(1.0 / k), (float)s0, chunk, partial.as<float2>(),
                 partial2.as<float2>(), nullptr, nullptr};
     float ms = 0.f;
-    for (int rep = 0; rep < 2; ++rep) {  // first launch warms, second is timed
-      cudaEventRecord(e0, st);
-      kF32X2Variants[v].direct(fast_trig, lofree, grid, st, a);
-      cudaEventRecord(e1, st);
-    }
-    cudaError_t e = cudaEventSynchronize(e1);
-    if (e == cudaSuccess) e = cudaGetLastError();
-    if (e != cudaSuccess) {
-      cudaEventDestroy(e0);
-      cudaEventDestroy(e1);
-      return cuda_status(e, "two-vector pair-kernel tuning", __FILE__, __LINE__);
-    }
-    g_launches.fetch_add(2, std::memory_order_relaxed);
-    cudaEventElapsedTime(&ms, e0, e1);
+    LUM_TRY(time_best([&] { kF32X2Variants[v].direct(fast_trig, lofree, grid, st, a); }, st,
+                      ev.e0, ev.e1, "two-vector pair-kernel tuning", &ms));
     if (ms < best) {
       best = ms;
       f32x2_variant = v;
     }
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  if (sym_allowed) {
+    LUM_TRY(sym_prepare(st));
+    for (int v = 1; v <= kNumSym2Variants; ++v) {
+      float ms = 0.f;
+      LUM_TRY(time_best(
+          [&] { sym2_launch(v, xz.as<double2>(), xz.as<double2>(), nullptr, nullptr, st); }, st,
+          ev.e0, ev.e1, "two-vector symmetric pair-kernel tuning", &ms));
+      if (ms < best) {
+        best = ms;
+        f32x2_sym = v;
+      }
+    }
+  }
   nsplit_x2 = ns_v[f32x2_variant];
   tuned_x2_ms = best;
-  std::lock_guard<std::mutex> lk(g_tune_mu);
-  g_tune_x2_cache[key] = f32x2_variant;
+  tune_store(key, f32x2_variant + 100 * f32x2_sym);
   return LUM_OK;
 }
 
@@ -1301,6 +1441,18 @@ lum_status OtfOperator::apply2(int precision, const double2* x, const double2* x
   const size_t slice = 3 * (size_t)n;
   if (precision == LUM_FP32) {
     if (f32x2_variant < 0) LUM_TRY(tune_f32_x2(st));
+    if (f32x2_sym && !has_substrate) {
+      if (ev0) cudaEventRecord(ev0, st);
+      sym2_launch(f32x2_sym, x, x2, skip, skip2, st);
+      LUM_CHECK_LAUNCH();
+      if (ev1) cudaEventRecord(ev1, st);
+      float2* s1 = sym_slots.as<float2>();
+      otf_epilogue2<float2, float2><<<epi_blocks, 256, 0, st>>>(
+          n, x, x2, inv_alpha.as<double2>(), s1, s1 + (size_t)sym_nb * slice, sym_nb, ell_w,
+          near_j.as<int>(), fcd32.as<float2>(), y, y2, skip, skip2);
+      LUM_CHECK_LAUNCH();
+      return LUM_OK;
+    }
     const F32X2VariantEntry& V = kF32X2Variants[f32x2_variant];
     const int ns = nsplit_x2;
     const int chunk = ((ntiles + ns - 1) / ns) * kOtfBlock;
@@ -1330,6 +1482,20 @@ lum_status OtfOperator::apply2(int precision, const double2* x, const double2* x
     otf_epilogue2<float2, float2><<<epi_blocks, 256, 0, st>>>(
         n, x, x2, inv_alpha.as<double2>(), part, part2, nparts, ell_w, near_j.as<int>(),
         fcd32.as<float2>(), y, y2, skip, skip2);
+    LUM_CHECK_LAUNCH();
+    return LUM_OK;
+  }
+  if (f64_sym && !has_substrate) {
+    if (!sym_slots2.p) LUM_TRY(sym_slots2.alloc(sym_slots.bytes));
+    double2 *s1 = sym_slots.as<double2>(), *s2 = sym_slots2.as<double2>();
+    if (ev0) cudaEventRecord(ev0, st);
+    otf_pairs_f64_sym2<<<sym_nitems, kSym64Threads, 0, st>>>(
+        n, pos64.as<double4>(), x, x2, k, 1.0 / k, s0, sym_items.as<int2>(), s1, s2, skip, skip2);
+    LUM_CHECK_LAUNCH();
+    if (ev1) cudaEventRecord(ev1, st);
+    otf_epilogue2<double2, double2><<<epi_blocks, 256, 0, st>>>(
+        n, x, x2, inv_alpha.as<double2>(), s1, s2, sym_nb, ell_w, near_j.as<int>(),
+        fcd64.as<double2>(), y, y2, skip, skip2);
     LUM_CHECK_LAUNCH();
     return LUM_OK;
   }
@@ -1415,6 +1581,33 @@ batch_pairs_f32(BatchGeom g, const double2* __restrict__ x, const int4* __restri
         n, g.hi + off, g.lo + off, g.hi + off, g.lo + off, x + 3 * (size_t)off, nullptr, one,
         one, one, (float)k, (float)(1.0 / k), (float)(k * k * k / (4.0 * kPi)), item.y, j0, j1,
         partial + (size_t)item.z * stride + 3 * (size_t)off, nullptr);
+  }
+}
+
+// The symmetric scheme over the batch: items (system, I, J), I <= J, the
+// superblock pairs of each system (pairs_f32_sym.cuh), written to per-system
+// slots laid out like the split partials, [superblock][3N] over the global
+// dipole range, so the batch epilogue sums sys_nb[s] of them per row.
+template <bool FAST, bool LOFREE, int MINB, int RP>
+__global__ void __launch_bounds__(SymShape<RP>::kThreads, MINB)
+batch_pairs_f32_sym(BatchGeom g, const double2* __restrict__ x, const int4* __restrict__ items,
+                    int nitems, unsigned* counters, const BatchFlags* __restrict__ flags,
+                    int skip_mode, float2* __restrict__ slots) {
+  __shared__ int s_item;
+  __shared__ float4 sS[6][32];
+  __shared__ float2 sAcc[SymShape<RP>::kWarps * 32 * 6];
+  __shared__ float sRed[32 * 6];
+  const size_t stride = 3 * (size_t)g.N;
+  for (int it; (it = batch_draw(counters, nitems, &s_item)) >= 0;) {
+    const int4 item = items[it];
+    const int s = item.x;
+    if (batch_skipped(flags, s, skip_mode)) continue;  // CTA-uniform
+    const int off = g.sys_off[s], n = g.sys_off[s + 1] - off;
+    const double k = g.sys_k[s];
+    sym_superblock_pair<FAST, LOFREE, RP, 1>(
+        n, g.hi + off, g.lo + off, x + 3 * (size_t)off, nullptr, (float)k,
+        (float)(k * k * k / (4.0 * kPi)), item.y, item.z, slots + 3 * (size_t)off, nullptr,
+        stride, sS, sAcc, sRed);
   }
 }
 
@@ -1593,6 +1786,101 @@ lum_status batch_near_fcd(BatchGeom& g, int use_fcd, DevBuf& near_j, DevBuf& fcd
   return LUM_OK;
 }
 
+// Builds of the batched symmetric kernel (g.sym32 = 1 + index): 2 rows per
+// thread at 2 CTAs per SM, or 4 rows per thread at 4 CTAs per SM.
+template <int MINB, int RP>
+static void batch_sym_launch_t(const BatchGeom& g, const double2* x, const BatchQueue& q,
+                               const BatchFlags* flags, int skip_mode, float2* slots,
+                               cudaStream_t st) {
+#define LUM_BSYM(F, L)                                                                       \
+  batch_pairs_f32_sym<F, L, MINB, RP><<<q.grid, SymShape<RP>::kThreads, 0, st>>>(            \
+      g, x, q.items.as<int4>(), q.nitems, q.counters.as<unsigned>(), flags, skip_mode, slots)
+  if (g.fast && g.lofree)
+    LUM_BSYM(true, true);
+  else if (g.fast)
+    LUM_BSYM(true, false);
+  else if (g.lofree)
+    LUM_BSYM(false, true);
+  else
+    LUM_BSYM(false, false);
+#undef LUM_BSYM
+}
+
+template <int MINB, int RP>
+static int batch_sym_occupancy_t(const BatchGeom& g) {
+  int occ = 1;
+  if (g.fast && g.lofree)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_pairs_f32_sym<true, true, MINB, RP>,
+                                                  SymShape<RP>::kThreads, 0);
+  else if (g.fast)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_pairs_f32_sym<true, false, MINB, RP>,
+                                                  SymShape<RP>::kThreads, 0);
+  else if (g.lofree)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_pairs_f32_sym<false, true, MINB, RP>,
+                                                  SymShape<RP>::kThreads, 0);
+  else
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &occ, batch_pairs_f32_sym<false, false, MINB, RP>, SymShape<RP>::kThreads, 0);
+  return std::max(1, occ);
+}
+
+namespace {
+struct BatchSymVariant {
+  const char* name;
+  void (*launch)(const BatchGeom&, const double2*, const BatchQueue&, const BatchFlags*, int,
+                 float2*, cudaStream_t);
+  int (*occupancy)(const BatchGeom&);
+};
+const BatchSymVariant kBatchSym[] = {
+    {"batch_sym_rows2_minb2", batch_sym_launch_t<2, 1>, batch_sym_occupancy_t<2, 1>},
+    {"batch_sym_rows4_minb4", batch_sym_launch_t<4, 2>, batch_sym_occupancy_t<4, 2>},
+};
+constexpr int kNumBatchSym = sizeof(kBatchSym) / sizeof(kBatchSym[0]);
+}  // namespace
+
+int batch_sym_variants() { return kNumBatchSym; }
+const char* batch_sym_name(int v) {
+  return (v >= 1 && v <= kNumBatchSym) ? kBatchSym[v - 1].name : "none";
+}
+int batch_sym_occupancy(const BatchGeom& g, int v) {
+  return kBatchSym[std::min(std::max(v, 1), kNumBatchSym) - 1].occupancy(g);
+}
+
+// Work list of the symmetric scheme: every superblock pair (I <= J) of every
+// system, ordered by decreasing cost (diagonal pairs count half).
+lum_status batch_queue_sym(const std::vector<int>& off, int slots, BatchQueue& q,
+                           std::vector<int>& nb, cudaStream_t st) {
+  const int K = (int)off.size() - 1;
+  nb.assign(K, 1);
+  struct It {
+    long cost;
+    int s, I, J;
+  };
+  std::vector<It> list;
+  for (int s = 0; s < K; ++s) {
+    const int n = off[s + 1] - off[s];
+    nb[s] = (n + kSymRows - 1) / kSymRows;
+    for (int I = 0; I < nb[s]; ++I)
+      for (int J = I; J < nb[s]; ++J) {
+        const long ri = std::min(kSymRows, n - I * kSymRows);
+        const long cj = std::min(kSymRows, n - J * kSymRows);
+        list.push_back({I == J ? ri * ri / 2 : ri * cj, s, I, J});
+      }
+  }
+  std::stable_sort(list.begin(), list.end(), [](const It& a, const It& b) { return a.cost > b.cost; });
+  std::vector<int4> items(list.size());
+  for (size_t t = 0; t < list.size(); ++t)
+    items[t] = make_int4(list[t].s, list[t].I, list[t].J, 0);
+  q.nitems = (int)items.size();
+  q.grid = std::max(1, std::min(q.nitems, slots));
+  LUM_TRY(q.items.alloc(sizeof(int4) * items.size()));
+  LUM_TRY(q.counters.alloc(2 * sizeof(unsigned)));
+  LUM_TRY_CUDA(cudaMemcpyAsync(q.items.p, items.data(), q.items.bytes, cudaMemcpyHostToDevice, st));
+  LUM_TRY_CUDA(cudaMemsetAsync(q.counters.p, 0, q.counters.bytes, st));
+  LUM_TRY_CUDA(cudaStreamSynchronize(st));  // the host item list is freed on return
+  return LUM_OK;
+}
+
 int batch_occupancy(const BatchGeom& g, int precision) {
   int occ = 1;
   if (precision == LUM_FP32) {
@@ -1668,6 +1956,16 @@ lum_status batch_apply(const BatchGeom& g, int precision, const double2* x, doub
   const int epi_blocks = (int)(((size_t)g.N * kEpiTPR + 255) / 256);
   const int4* items = q.items.as<int4>();
   unsigned* cnt = q.counters.as<unsigned>();
+  if (precision == LUM_FP32 && g.sym32 && g.qsym) {
+    float2* part = static_cast<float2*>(partial);
+    kBatchSym[std::min(g.sym32, kNumBatchSym) - 1].launch(g, x, *g.qsym, flags, skip_mode, part,
+                                                           st);
+    LUM_CHECK_LAUNCH();
+    batch_epilogue<float2, float2><<<epi_blocks, 256, 0, st>>>(g, x, part, g.sys_nb, g.fcd32,
+                                                               flags, skip_mode, y);
+    LUM_CHECK_LAUNCH();
+    return LUM_OK;
+  }
   if (precision == LUM_FP32) {
     float2* part = static_cast<float2*>(partial);
 #define LUM_BATCH_F32(F, L)                                                                 \

@@ -14,8 +14,10 @@
 // with m = (-r, -r, +r) and the self term (i == j) included, as the
 // reference's periodic branch does.  The epilogue (otf.cu) adds alpha^-1 x.
 //
-// Entries are padded to 10 complex numbers so an FP32 entry is five 16-byte
-// loads (FP64: ten).  The tables are O(N) in size and stay L2-resident.
+// The periodic tensor is symmetric, so an entry holds its six distinct
+// components (xx xy xz yy yz zz; kSym below maps (p, q) to a slot): an FP32
+// entry is three 16-byte loads, an FP64 entry six.  The tables are O(N) in
+// size and stay L2-resident.
 #include "lumina_internal.cuh"
 #include "device_physics.cuh"
 

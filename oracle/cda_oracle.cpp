@@ -1029,6 +1029,49 @@ int orc_matvec_onthefly_rows(int n, const double* pos, const double* alpha, cons
   return 0;
 }
 
+// Rows [row0, row1) of matvec_on_the_fly with every optional term (Ewald
+// lattice, Bloch vector, Fresnel image), the loop of otf_mv above restricted
+// to a row range: bounded samples of the periodic operator at full size.
+int orc_matvec_onthefly_rows_ex(int n, const double* pos, const double* alpha, const double* x,
+                                double k, int use_fcd, double cell, const orc_lattice* lat,
+                                const double* kb, const orc_substrate* subs, int row0, int row1,
+                                double* y, int nthreads) {
+  std::vector<C> inv;
+  if (!prepare_inv_alpha(n, alpha, inv)) return 6;
+  Lattice L;
+  if (lat) L = to_lat(lat);
+  Substrate S;
+  if (subs) S = Substrate{subs->z_interface, subs->refl_re, subs->refl_im};
+  OtfCtx o{n, pos, inv.data(), make_cfg(k, use_fcd, cell, lat ? &L : nullptr, kb, subs ? &S : nullptr),
+           set_threads(nthreads)};
+  const C* xc = reinterpret_cast<const C*>(x);
+  C* yc = reinterpret_cast<C*>(y);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(o.nthreads)
+  for (int i = row0; i < row1; ++i) {
+    C yi[3] = {cc(0.0), cc(0.0), cc(0.0)};
+    const C* ia = o.inv_alpha + 9 * (size_t)i;
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) yi[a] = add(yi[a], mul(ia[3 * a + b], xc[3 * i + b]));
+    const double* ri = pos + 3 * (size_t)i;
+    for (int j = 0; j < n; ++j) {
+      T3 dg, sg;
+      bool hd, hs;
+      pair_blocks(o.P, ri, pos + 3 * (size_t)j, i == j, dg, &hd, sg, &hs);
+      if (hd)
+        for (int a = 0; a < 3; ++a)
+          for (int b = 0; b < 3; ++b) yi[a] = sub(yi[a], mul(dg[a][b], xc[3 * j + b]));
+      if (hs) {
+        C rr = C{o.P.sub->refl_re, o.P.sub->refl_im};
+        C m[3] = {neg(rr), neg(rr), rr};
+        for (int a = 0; a < 3; ++a)
+          for (int b = 0; b < 3; ++b) yi[a] = sub(yi[a], mul(mul(m[b], sg[a][b]), xc[3 * j + b]));
+      }
+    }
+    for (int c = 0; c < 3; ++c) yc[3 * (i - row0) + c] = yi[c];
+  }
+  return 0;
+}
+
 // solve_gmres over a dense matrix (iterative.rs:33-160 with the matrix matvec
 // closure of iterative.rs:214-216 / cpu.rs:64-70).
 int orc_gmres_dense(int dim, const double* A, const double* b, double tol, int max_iter,

@@ -77,6 +77,9 @@ def _load():
                                         ctypes.c_void_p, _dp, ctypes.c_void_p, _dp, c_int]),
         "orc_matvec_onthefly_rows": (c_int, [c_int, _dp, _dp, _dp, c_double, c_int, c_double,
                                              c_int, c_int, _dp, c_int]),
+        "orc_matvec_onthefly_rows_ex": (c_int, [c_int, _dp, _dp, _dp, c_double, c_int,
+                                                c_double, ctypes.c_void_p, _dp,
+                                                ctypes.c_void_p, c_int, c_int, _dp, c_int]),
         "orc_gmres_dense": (c_int, [c_int, _dp, _dp, c_double, c_int, c_int, _dp, _ip, _ip,
                                     _dp, c_int]),
         "orc_gmres_onthefly": (c_int, [c_int, _dp, _dp, _dp, c_double, c_int, c_double,
@@ -257,6 +260,24 @@ def matvec_onthefly(pos, alpha, x, k, use_fcd=False, cell_size=3.0, lattice=None
     rc = lib().orc_matvec_onthefly(n, _p(pos), _p(a.view(np.float64)), _p(x.view(np.float64)),
                                    k, int(use_fcd), cell_size, _ref(ls), _p(_vec(k_bloch)),
                                    _ref(ss), _p(y.view(np.float64)), nthreads)
+    if rc != 0:
+        raise ValueError("singular polarisability")
+    return y
+
+
+def matvec_onthefly_rows_ex(pos, alpha, x, k, use_fcd, cell_size, row0, row1, lattice=None,
+                            k_bloch=(0, 0, 0), substrate=None, nthreads=0):
+    """Rows [row0, row1) of matvec_onthefly with the lattice / substrate terms."""
+    pos = _vec(pos).reshape(-1, 3)
+    n = pos.shape[0]
+    a = _alpha_arr(alpha, n)
+    x = np.ascontiguousarray(np.asarray(x, np.complex128))
+    y = np.zeros(3 * (row1 - row0), np.complex128)
+    ls, ss = _lat(lattice), _sub(substrate)
+    rc = lib().orc_matvec_onthefly_rows_ex(n, _p(pos), _p(a.view(np.float64)),
+                                           _p(x.view(np.float64)), k, int(use_fcd), cell_size,
+                                           _ref(ls), _p(_vec(k_bloch)), _ref(ss), row0, row1,
+                                           _p(y.view(np.float64)), nthreads)
     if rc != 0:
         raise ValueError("singular polarisability")
     return y

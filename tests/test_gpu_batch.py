@@ -165,3 +165,29 @@ def test_batch_rejects_invalid_input(backend):
     bad[2] = [np.nan, 0.0, 0.0]
     with pytest.raises(lb.InvalidGeometry):
         backend.create_batch([(bad, inv, 0.01, 1.5)])
+
+
+@pytest.mark.parametrize("variant", ["1", "2"])
+def test_batch_symmetric_scheme_matches_oracle(backend, rng, monkeypatch, variant):
+    """The symmetric FP32 scheme over the batch (each unordered pair once per
+    system, superblock pairs drawn from one work list; LUMINA_BATCH_SYM=v
+    forces build v): systems of 200-1400 dipoles, so superblock edges and
+    diagonal blocks are crossed; every system against the oracle, and the
+    FP32+refine solve against the FP64 one."""
+    monkeypatch.setenv("LUMINA_BATCH_SYM", variant)
+    w = small_batch(count=3, seed=7, n_range=(200, 1400))
+    systems, specs = batch_inputs(w)
+    with backend.create_batch(specs) as B:
+        x = rand_vec(rng, B.dim)
+        y32 = B.split(B.matvec(x, "fp32"))
+        xs = B.split(x)
+        for s, (p, a, k, cell, _) in enumerate(systems):
+            y_ref = orc.matvec_onthefly(p, a, xs[s], k, True, cell)
+            assert rel_err(y32[s], y_ref) < 2e-5, (variant, s)
+        b = np.concatenate([lb.incident_field(p, k, inc) for p, _, k, _, inc in systems])
+        x32, i32 = B.solve(b, 1e-10, 5000, 30, "fp32_refine")
+        x64, i64 = B.solve(b, 1e-10, 5000, 30, "fp64")
+        for s, ((p, inv, k, cell), (_, _, _, _, inc)) in enumerate(zip(specs, systems)):
+            c32 = lb.cross_sections(p, inv, B.split(x32)[s], k, inc)[0]
+            c64 = lb.cross_sections(p, inv, B.split(x64)[s], k, inc)[0]
+            assert abs(c32 - c64) <= 1e-6 * abs(c64), (variant, s)

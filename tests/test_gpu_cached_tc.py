@@ -191,3 +191,52 @@ def test_rhs_batch_on_the_fly_session(backend):
         for q in range(len(dirs)):
             x1, _ = S.solve(rhs[q], 1e-10, 5000, 30, "fp64")
             assert rel_err(x[3 * w.n * q:3 * w.n * (q + 1)], x1) < 1e-7
+
+
+def test_tensor_wait_limit_reports_timeout_and_context_recovers(backend, rng, monkeypatch):
+    """A pipeline wait that never completes (the first CTA's split warps
+    withhold one arrival, LUMINA_TC_WITHHOLD_SPLIT=1) gives up after the
+    launch's wait limit (LUMINA_TC_WAIT_CYCLES, here ~10 ms of SM clocks):
+    the product returns TIMEOUT, and the next product on the same session is
+    exact again."""
+    dim, nrhs = 999, 8
+    A = _rand_matrix(rng, dim)
+    X = _rand_block(rng, dim, nrhs)
+    Y_ref = A.astype(np.complex64).astype(np.complex128) @ X
+    with backend.create_session(dim, "fp32") as s:
+        s.upload_matrix(A)
+        monkeypatch.setenv("LUMINA_TC_WAIT_CYCLES", "20000000")
+        monkeypatch.setenv("LUMINA_TC_WITHHOLD_SPLIT", "1")
+        with pytest.raises(lb.DeviceTimeout):
+            s.matmul(X, "tensor")
+        monkeypatch.delenv("LUMINA_TC_WITHHOLD_SPLIT")
+        Y = s.matmul(X, "tensor")  # short limit kept: a healthy product meets it
+        monkeypatch.delenv("LUMINA_TC_WAIT_CYCLES")
+        Y2 = s.matmul(X, "tensor")
+    assert rel_err(Y, Y_ref) < 1e-5
+    assert rel_err(Y2, Y_ref) < 1e-5
+
+
+def test_rhs_batch_reports_tensor_timeout(backend, monkeypatch):
+    """The right-hand-side batch on FP32 cached storage reads the tensor-core
+    status after every restart cycle: a product that gave up a wait ends the
+    solve with TIMEOUT instead of a wrong solution, and a later solve on the
+    same session converges."""
+    pos = discretise_primitive(Sphere((0.0, 0.0, 0.0), 6.0), 2.0)
+    w = configs.au_workload("s", pos, 2.0, 520.0)
+    inv = lb.invert_polarisability(w.alpha)
+    dirs = _directions(4)
+    rhs = np.concatenate([orc.incident_field(w.positions, w.k, d, e) for d, e in dirs])
+    with backend.assemble_and_create_session(w.positions, w.k, inv, True, 2.0,
+                                             precision="fp32") as S:
+        B = S.rhs_batch(len(dirs))
+        monkeypatch.setenv("LUMINA_TC_WAIT_CYCLES", "20000000")
+        monkeypatch.setenv("LUMINA_TC_WITHHOLD_SPLIT", "1")
+        with pytest.raises(lb.DeviceTimeout):
+            B.solve(rhs, 1e-10, 5000, 30, "fp32_refine")
+        monkeypatch.delenv("LUMINA_TC_WITHHOLD_SPLIT")
+        monkeypatch.delenv("LUMINA_TC_WAIT_CYCLES")
+        x, info = B.solve(rhs, 1e-10, 5000, 30, "fp32_refine")
+        B.close()
+    assert all(i["converged"] == 1 for i in info)
+    assert np.all(np.isfinite(x))
