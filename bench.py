@@ -830,8 +830,16 @@ def _bench_cached(args, bk, stream, torch, lb, configs):
             peaks = _json.load(f)
     except (OSError, ValueError):
         pass
+    # MEASURED_PEAKS.json (written per pool) when present, else the pool's
+    # earlier measurement (6.65 TB/s, 1.59 PFLOP/s bf16); the line says which
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     tf32_peak = float(peaks.get("bf16_tflops", 1590.0)) / 2.0  # dense TF32 = half of BF16
+    hbm_src = "MEASURED_PEAKS.json hbm_gbs; of measured" if "hbm_gbs" in peaks else \
+        "no MEASURED_PEAKS.json: the pool's earlier copy measurement, 6650 GB/s; of fallback"
+    tf32_src = ("TF32 dense = MEASURED_PEAKS.json bf16_tflops / 2; of measured"
+                if "bf16_tflops" in peaks else
+                "no MEASURED_PEAKS.json: TF32 dense = 1590 / 2 TFLOP/s (earlier bf16 "
+                "measurement on this pool); of fallback")
     size = tuple(float(v) for v in (args.size if args.size != "60,50,10" else "30,20,10").split(","))
     w = configs.cuboid_au(size, 1.0, 520.0)
     n, dim = w.n, 3 * w.n
@@ -867,6 +875,17 @@ def _bench_cached(args, bk, stream, torch, lb, configs):
                                                   stream.cuda_stream))
     torch.cuda.synchronize()
     err = float(torch.max(torch.abs(Y - Yc)) / torch.max(torch.abs(Yc)))
+    # e2e: the same GEMV through the host-array call (vector in, product out)
+    x1h = x1.cpu().numpy()
+    S.matvec(x1h, "fp32")
+    e2e_ms = []
+    for _ in range(reps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        S.matvec(x1h, "fp32")
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_gemv = statistics.median(e2e_ms)
     a_bytes = 8.0 * dim * dim
     cflops = 8.0 * dim * dim * R            # complex multiply-adds x 8 real flops
     tc_flops = 3.0 * cflops                 # three TF32 products per operand pair
@@ -883,7 +902,7 @@ def _bench_cached(args, bk, stream, torch, lb, configs):
             "roofline": {"bound": "hbm", "kernel": "gemv_part<float2> + gemv_reduce",
                          "achieved": a_bytes / (ms_gemv * 1e-3) / 1e9, "peak": hbm_peak,
                          "unit": "GB/s", "frac": a_bytes / (ms_gemv * 1e-3) / 1e9 / hbm_peak,
-                         "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs; of measured"},
+                         "traffic": None, "peak_source": hbm_src},
             "tensor_product": {
                 "kernel": "cgemm_tf32x3_kernel", "nrhs": R, "ms": ms_tc,
                 "complex_tflops": cflops / (ms_tc * 1e-3) / 1e12,
@@ -893,11 +912,12 @@ def _bench_cached(args, bk, stream, torch, lb, configs):
                 "hbm_gbs": a_bytes / (ms_tc * 1e-3) / 1e9,
                 "hbm_frac": a_bytes / (ms_tc * 1e-3) / 1e9 / hbm_peak,
                 "bound_ms": max(a_bytes / (hbm_peak * 1e9), tc_flops / (tf32_peak * 1e12)) * 1e3,
-                "peak_source": "TF32 dense = MEASURED_PEAKS.json bf16_tflops / 2; of measured",
+                "peak_source": tf32_src,
                 "speedup_vs_cuda_cores": ms_cc / ms_tc, "cuda_cores_ms": ms_cc,
                 "rel_diff_vs_cuda_cores": err,
                 "gemv_equivalent_ms": ms_gemv * R},
-            "e2e": None}
+            "e2e": {"value": a_bytes / (e2e_gemv * 1e-3) / 1e9, "unit": "GB/s (GEMV)",
+                    "h2d_bytes_per_step": dim * 16, "d2h_bytes_per_step": dim * 16}}
 
 
 def _incidence_set(m):
@@ -943,6 +963,9 @@ def _bench_directions(args, bk, stream, torch, lb, configs):
     torch.cuda.synchronize()
     t_tc = time.perf_counter() - t0
     x_tc = x_dev.cpu().numpy()
+    t0 = time.perf_counter()
+    B.solve(rhs, tol, max_iter, 30, "fp32_refine")  # e2e: host arrays in and out
+    t_e2e = time.perf_counter() - t0
     B.close()
     C.close()
     O = bk.create_onthefly_session(w.positions, inv, w.k, True, 1.0)
@@ -978,7 +1001,9 @@ def _bench_directions(args, bk, stream, torch, lb, configs):
             "iterations": {"min": min(its), "max": max(its)},
             "onthefly_two_at_a_time": {"value": n * R / t_otf, "seconds": t_otf,
                                        "speedup_of_tensor_path": t_otf / t_tc},
-            "max_cext_rel_diff_vs_onthefly": err, "e2e": None}
+            "max_cext_rel_diff_vs_onthefly": err,
+            "e2e": {"value": n * R / t_e2e, "unit": UNIT, "h2d_bytes_per_step": int(rhs.nbytes),
+                    "d2h_bytes_per_step": int(rhs.nbytes)}}
 
 
 def _bench_fft(args, bk, stream, torch, lb, configs):
@@ -1037,6 +1062,34 @@ def _bench_fft(args, bk, stream, torch, lb, configs):
         apply_ms[prec] = ms / 20
     cfg = F.kernel_config()
     F.close()
+    # e2e: the solver's FFT branch with host arrays over the same wavelengths
+    solver = lb.CdaSolver(backend=bk, iterative_threshold=0, use_fcd=True, cell_size=1.0,
+                          matrix_memory_budget=0, precision="fp32_refine", use_fft=True)
+    params = lb.SimulationParams(solver_tolerance=args.tol, max_iterations=args.max_iter)
+    ds = [lb.DipoleSet(w.positions, w.alpha) for w in per]
+    solver.compute_cross_sections(ds[0], lams[0], params)  # warm
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i, lam in enumerate(lams):
+        solver.compute_cross_sections(ds[i], lam, params)
+    torch.cuda.synchronize()
+    t_e2e = time.perf_counter() - t0
+    solver.close()
+    # roofline of one FP32 application: the pass structure's L2 traffic -- six
+    # axis passes (three forward, three inverse) and the spectral product each
+    # read and write the three-component grid (M complex FP32 per component),
+    # and the product reads the six kernel spectra; no credit is taken for the
+    # lines the passes skip, so this over-counts and the fraction is an upper
+    # bound
+    size = [float(v) for v in args.size.split(",")]
+    m = 1
+    for L in size:
+        c = 1
+        while c < 2 * int(round(L)) - 1:
+            c *= 2
+        m *= c
+    fft_bytes = 6.0 * m * 8.0 + 7.0 * 2.0 * 3.0 * m * 8.0
+    l2_peak = bk.measure_l2_peak()
     nl = len(rows)
     return {"metric": "dipole-solves/s at N=30k through the FFT (block-Toeplitz) operator, "
                       "FP32+refine", "value": n * nl / (t32 * 1e-3), "unit": UNIT,
@@ -1046,7 +1099,19 @@ def _bench_fft(args, bk, stream, torch, lb, configs):
             "fp64_plain": {"value": n * nl / (t64 * 1e-3), "speedup_same_solves": t64 / t32},
             "apply_ms": apply_ms,
             "max_cext_rel_err_vs_onthefly_fp64": max(r["cext_rel_err_vs_onthefly"] for r in rows),
-            "per_wavelength": rows, "kernel_config": cfg, "e2e": None}
+            "per_wavelength": rows, "kernel_config": cfg,
+            "roofline": {"bound": "l2", "kernel": "fft_lines + fft_spectral_product",
+                         "achieved": fft_bytes / (apply_ms["fp32"] * 1e-3) / 1e9,
+                         "peak": l2_peak, "unit": "GB/s",
+                         "frac": fft_bytes / (apply_ms["fp32"] * 1e-3) / 1e9 / l2_peak,
+                         "bytes_model": f"{fft_bytes / 1e6:.0f} MB per FP32 application: 7 "
+                                        f"passes x read+write of 3 x {m} complex FP32 + 6 "
+                                        f"spectra (skipped lines not credited: upper bound)",
+                         "peak_source": "L2 read microbenchmark in this run "
+                                        "(lum_measure_l2_peak); of measured", "traffic": None},
+            "e2e": {"value": n * nl / t_e2e, "unit": UNIT,
+                    "h2d_bytes_per_step": n * 3 * 8 + n * 9 * 16,
+                    "d2h_bytes_per_step": 3 * n * 16}}
 
 
 def _bench_fields(args, bk, stream, torch, lb, configs, fp64_peak):
