@@ -1372,9 +1372,9 @@ MSURF_SAMPLE_NM = ",".join(f"{500.0 + 50.0 * i:g}" for i in range(11))
 def _bench_metasurface(args, bk, stream, torch, lb, configs):
     from oracle import oracle as orc
     lams = wavelength_list(args, MSURF_SAMPLE_NM)
-    # 4 nm lattice: ~5.4k dipoles per cell, the size the metasurface
-    # configuration quotes (~4,900); --spacing 2 gives ~41k.
-    spacing = args.spacing or 4.0
+    # the configuration's 2 nm lattice: 41,181 dipoles per cell (its "~4,900"
+    # is the 4 nm lattice's count, 5,379: --spacing 4)
+    spacing = args.spacing or 2.0
     tol, max_iter = args.tol, max(args.max_iter, 20000)
     l2_peak = bk.measure_l2_peak()
     rows, parity, counts = [], None, []

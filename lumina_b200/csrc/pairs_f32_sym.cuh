@@ -13,15 +13,16 @@
 // two halves of a float2 as in pairs_f32x2.cuh (warp w, row pair p: rows
 // I*kSymRows + 64*RP*w + 64*p + {lane, lane + 32}), with their positions,
 // moments x_i and row sums in registers; the CTA has kSymRows / (2*RP)
-// threads.  The sources of J are staged 32 at a time in shared memory; in
-// step s of a group, lane l pairs its rows with source (l + s) mod 32
+// threads (RP = 4: 64).  The sources of J are staged 32 at a time in shared
+// memory; in step s of a group, lane l pairs its rows with source (l + s) mod 32
 // (conflict-free: consecutive lanes read consecutive entries).  The
 // source-side sums travel with the sources: after each step every lane
 // passes its source accumulator (summed over its 2*RP rows) to lane l - 1,
 // so after 32 steps lane l holds the sum for source l over the warp's rows.
 // The warps' sums are then added in warp order.  RP = 2 halves the shared
 // loads and shuffles per pair and gives each step two independent tensor
-// evaluations to interleave, at the cost of registers.
+// evaluations to interleave, at the cost of registers; UNR = 2 unrolls the
+// step loop so that one step's shuffles overlap the next step's tensor.
 //
 // NV = 2 applies the operator to two vectors at once (forward + adjoint,
 // two polarisations): the tensor scalars are evaluated once per unordered
@@ -120,7 +121,7 @@ __device__ __forceinline__ void sym_contract(float2 dx, float2 dy, float2 dz, fl
 // comes from the caller: sS [6 + 3 (NV - 1)][32] staged sources, sAcc
 // [warps][32][6 NV] per-warp source sums, sRed [32][6 NV] the diagonal
 // hand-off.
-template <bool FAST, bool LOFREE, int RP, int NV>
+template <bool FAST, bool LOFREE, int RP, int NV, int UNR = 1>
 __device__ __forceinline__ void sym_superblock_pair(
     int n, const float4* __restrict__ obs_hi, const float4* __restrict__ obs_lo,
     const double2* __restrict__ xa_v, const double2* __restrict__ xb_v, float k, float s0,
@@ -214,7 +215,7 @@ __device__ __forceinline__ void sym_superblock_pair(
     for (int v = 0; v < NV; ++v)
 #pragma unroll
       for (int c = 0; c < 6; ++c) sacc[v][c] = make_float2(0.f, 0.f);
-#pragma unroll 1
+#pragma unroll UNR
     for (int s = 0; s < 32; ++s) {
       const int src = (lane + s) & 31;
       const float4 S0 = sS[0][src], S1 = sS[1][src], S2 = sS[2][src], S3 = sS[3][src],
@@ -321,7 +322,7 @@ __device__ __forceinline__ void sym_superblock_pair(
     }
 }
 
-template <bool FAST, bool LOFREE, int MINB, int RP>
+template <bool FAST, bool LOFREE, int MINB, int RP, int UNR = 1>
 __global__ void __launch_bounds__(SymShape<RP>::kThreads, MINB)
 otf_pairs_f32_sym(int n, const float4* __restrict__ obs_hi, const float4* __restrict__ obs_lo,
                   const double2* __restrict__ x, float k, float s0,
@@ -332,8 +333,9 @@ otf_pairs_f32_sym(int n, const float4* __restrict__ obs_hi, const float4* __rest
   __shared__ float2 sAcc[SymShape<RP>::kWarps * 32 * 6];
   __shared__ float sRed[32 * 6];
   const int2 it = items[blockIdx.x];
-  sym_superblock_pair<FAST, LOFREE, RP, 1>(n, obs_hi, obs_lo, x, nullptr, k, s0, it.x, it.y,
-                                           slots, nullptr, 3 * (size_t)n, sS, sAcc, sRed);
+  sym_superblock_pair<FAST, LOFREE, RP, 1, UNR>(n, obs_hi, obs_lo, x, nullptr, k, s0, it.x,
+                                                it.y, slots, nullptr, 3 * (size_t)n, sS, sAcc,
+                                                sRed);
 }
 
 // Two vectors (see NV above).  A vector whose skip flag is set is left out;

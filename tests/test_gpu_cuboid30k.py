@@ -67,7 +67,7 @@ def test_cuboid30k_tuned_operator_rows_match_oracle(backend, cuboid, monkeypatch
     assert _err(_rows(y64), yref) < 1e-12
 
 
-@pytest.mark.parametrize("variant", ("1", "3"))
+@pytest.mark.parametrize("variant", ("1", "3", "6", "7"))
 def test_cuboid30k_symmetric_builds_match_oracle(backend, cuboid, monkeypatch, variant):
     monkeypatch.setenv("LUMINA_F32_SYM", variant)
     monkeypatch.setenv("LUMINA_F64_SYM", "1")
