@@ -578,7 +578,10 @@ def main():
                 "rel_residual": info_lam[i]["rel_residual"],
                 "converged": info_lam[i]["converged"], "c_ext": cs32[i][0], "c_abs": cs32[i][1]}
                for i in sorted(ms_lam)]
-    pin0 = oracle_pin[0] if oracle_pin else {}
+    # the headline figures quote the 520 nm solve, the one the reference arm
+    # repeats live; the other fixture wavelengths are in oracle_pin
+    pin0 = next((p for p in (oracle_pin or []) if p["wavelength_nm"] == 520.0),
+                (oracle_pin or [{}])[0])
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_max_s * 1e3 / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
