@@ -293,6 +293,10 @@ LUM_API int lum_batch_solve(lum_batch* b, const double* rhs, double tol, int max
 LUM_API int lum_batch_solve_device(lum_batch* b, const void* rhs_dev, void* x_dev, double tol,
                                    int max_iter, int restart, int mode, lum_solve_info* info);
 LUM_API int lum_batch_set_stream(lum_batch* b, void* stream);
+/* The kernels a cluster batch runs, as "key=value" tokens: the FP32 pair
+ * scheme chosen at creation (split work list or a symmetric build) and its
+ * work-list sizes.  No counterpart in the reference. */
+LUM_API int lum_batch_kernel_config(lum_batch* b, char* buf, size_t len);
 /* No counterpart in the reference, which solves one incidence at a time
  * (cda/mod.rs:238-391): a batch of nrhs right-hand sides of one session's
  * operator (incidence directions, polarisations), solved by lum_batch_solve

@@ -134,6 +134,7 @@ SIGNATURES = {
     "lum_batch_solve_device": (c_int, [c_void_p, c_void_p, c_void_p, c_double, c_int, c_int,
                                        c_int, POINTER(LumSolveInfo)]),
     "lum_batch_set_stream": (c_int, [c_void_p, c_void_p]),
+    "lum_batch_kernel_config": (c_int, [c_void_p, c_char_p, c_size_t]),
     "lum_batch_create_rhs": (c_int, [c_void_p, c_int, POINTER(c_void_p)]),
     "lum_batch_info": (c_int, [c_void_p] + [POINTER(c_int)] * 9),
     "lum_batch_destroy": (c_int, [c_void_p]),

@@ -502,6 +502,19 @@ class CudaBatch:
         _raise(rc, "batch solve_device")
         return d
 
+    def kernel_config(self) -> dict:
+        """The FP32 pair scheme this batch chose and its work-list sizes."""
+        buf = ctypes.create_string_buffer(512)
+        _raise(self._lib.lum_batch_kernel_config(self._h, buf, 512), "batch kernel_config")
+        out = {}
+        for tok in buf.value.decode().split():
+            key, _, val = tok.partition("=")
+            try:
+                out[key] = int(val)
+            except ValueError:
+                out[key] = val
+        return out
+
     def info(self) -> dict:
         vals = [c_int(0) for _ in range(9)]
         _raise(self._lib.lum_batch_info(self._h, *[byref(v) for v in vals]), "batch info")

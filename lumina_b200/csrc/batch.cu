@@ -1035,6 +1035,22 @@ int lum_batch_info(lum_batch* B, int* n_systems, int* n_dipoles, int* ell_width,
   return LUM_OK;
 }
 
+int lum_batch_kernel_config(lum_batch* B, char* buf, size_t len) {
+  if (bad_arg(B, "batch") || bad_arg(buf, "buf") || len == 0) return LUM_ERR_INVALID;
+  const BatchGeom& g = B->g;
+  snprintf(buf, len, "kind=%s fp32_scheme=%s sym32=%d items32=%d grid32=%d items64=%d grid64=%d "
+           "minb32=%d lofree=%d fast_trig=%d",
+           B->src ? "rhs" : "clusters", g.sym32 ? "symmetric" : "split",
+           g.sym32, g.sym32 ? B->qsym.nitems : B->q32.nitems,
+           g.sym32 ? B->qsym.grid : B->q32.grid, B->q64.nitems, B->q64.grid, g.minb32, g.lofree,
+           g.fast);
+  if (g.sym32) {
+    const size_t used = strlen(buf);
+    if (used + 1 < len) snprintf(buf + used, len - used, " sym_variant=%s", batch_sym_name(g.sym32));
+  }
+  return LUM_OK;
+}
+
 int lum_batch_matvec_device(lum_batch* B, int precision, const void* x_dev, void* y_dev) {
   if (bad_arg(B, "batch") || bad_arg(x_dev, "x") || bad_arg(y_dev, "y")) return LUM_ERR_INVALID;
   if (precision != LUM_FP32 && precision != LUM_FP64) {

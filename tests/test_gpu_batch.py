@@ -178,6 +178,8 @@ def test_batch_symmetric_scheme_matches_oracle(backend, rng, monkeypatch, varian
     w = small_batch(count=3, seed=7, n_range=(200, 1400))
     systems, specs = batch_inputs(w)
     with backend.create_batch(specs) as B:
+        cfg = B.kernel_config()
+        assert cfg["fp32_scheme"] == "symmetric" and cfg["sym32"] == int(variant)
         x = rand_vec(rng, B.dim)
         y32 = B.split(B.matvec(x, "fp32"))
         xs = B.split(x)
