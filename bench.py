@@ -368,6 +368,7 @@ def main():
     n = base.n
     bk = lb.CudaBackend(local)
     fp32_peak, fp64_peak = bk.measure_fma_peak()
+    fma2_peak = bk.measure_fma2_peak()
     # one dedicated stream for torch's events/copies and the library's kernels
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
@@ -550,6 +551,8 @@ def main():
             "traffic": _traffic_from_profiles(kname), "launches": k32, "applications": real32,
             "avg_launch_ms": avg32, "flops_per_launch": pairs * FLOPS_PER_PAIR,
             "kernel_config": kcfg,
+            "packed_fma2_peak_tflops": fma2_peak / 1e3,
+            "frac_of_packed_fma2_peak": achieved / (fma2_peak / 1e3) if fma2_peak else None,
             "fp64_kernel": {"kernel": k64name, "launches": k64, "applications": real64,
                             "avg_launch_ms": avg64, "achieved_tflops": a64,
                             "peak_tflops": fp64_peak / 1e3,

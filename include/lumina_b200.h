@@ -419,6 +419,10 @@ LUM_API int lum_measure_fma_peak(lum_ctx* ctx, double* fp32_gflops, double* fp64
  * periodic operator: GB/s on the context's device.  No counterpart in the
  * reference. */
 LUM_API int lum_measure_l2_peak(lum_ctx* ctx, double* gbs);
+/* The same FMA-chain microbenchmark with packed f32x2 FMAs (the instruction
+ * the FP32 pair kernels use): FP32 GFLOP/s.  No counterpart in the
+ * reference. */
+LUM_API int lum_measure_fma2_peak(lum_ctx* ctx, double* gflops);
 
 /* ---- allocation-free matvec ---------------------------------------------- */
 /* No counterpart in the reference.  For callers that cannot let a library

@@ -115,6 +115,7 @@ SIGNATURES = {
     "lum_session_kernel_config": (c_int, [c_void_p, c_char_p, c_size_t]),
     "lum_measure_fma_peak": (c_int, [c_void_p, POINTER(c_double), POINTER(c_double)]),
     "lum_measure_l2_peak": (c_int, [c_void_p, POINTER(c_double)]),
+    "lum_measure_fma2_peak": (c_int, [c_void_p, POINTER(c_double)]),
     "lum_near_field": (c_int, [c_void_p, c_int, _dp, _dp, c_double, _dp, _dp, c_double, c_int,
                                _dp, c_void_p, c_void_p]),
     "lum_near_field_map": (c_int, [c_void_p, c_int, _dp, _dp, c_double, _dp, _dp, c_double,

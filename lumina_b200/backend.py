@@ -695,6 +695,12 @@ class CudaBackend:
         _raise(self._lib.lum_measure_fma_peak(self._h, byref(f32), byref(f64)), "fma peak")
         return f32.value, f64.value
 
+    def measure_fma2_peak(self):
+        """FP32 GFLOP/s of packed f32x2 FMA chains."""
+        g = c_double(0.0)
+        _raise(self._lib.lum_measure_fma2_peak(self._h, byref(g)), "fma2 peak")
+        return g.value
+
     def measure_l2_peak(self):
         """L2 read bandwidth (GB/s) measured by a 16-byte-load kernel."""
         g = c_double(0.0)

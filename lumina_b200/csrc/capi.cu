@@ -74,6 +74,28 @@ __global__ void fma_chain(T* out, int iters, T a, T b) {
   if (s == (T)-12345.678) out[0] = s;  // keeps the chain live; never true
 }
 
+// Packed FP32 variant: eight float2 chains of f32x2 FMAs (the instruction the
+// FP32 pair kernels are built from).
+__global__ void fma2_chain(float* out, int iters, float a, float b) {
+  const float t = (float)threadIdx.x * 1e-7f;
+  float2 x0 = make_float2(t, t + 0.5f), x1 = make_float2(t + 1.f, t + 1.5f),
+         x2 = make_float2(t + 2.f, t + 2.5f), x3 = make_float2(t + 3.f, t + 3.5f),
+         x4 = make_float2(t + 4.f, t + 4.5f), x5 = make_float2(t + 5.f, t + 5.5f),
+         x6 = make_float2(t + 6.f, t + 6.5f), x7 = make_float2(t + 7.f, t + 7.5f);
+  const float2 A = make_float2(a, a), B = make_float2(b, b);
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      x0 = __ffma2_rn(x0, A, B); x1 = __ffma2_rn(x1, A, B); x2 = __ffma2_rn(x2, A, B);
+      x3 = __ffma2_rn(x3, A, B); x4 = __ffma2_rn(x4, A, B); x5 = __ffma2_rn(x5, A, B);
+      x6 = __ffma2_rn(x6, A, B); x7 = __ffma2_rn(x7, A, B);
+    }
+  }
+  const float s = x0.x + x1.x + x2.x + x3.x + x4.x + x5.x + x6.x + x7.x + x0.y + x1.y + x2.y +
+                  x3.y + x4.y + x5.y + x6.y + x7.y;
+  if (s == -12345.678f) out[0] = s;  // keeps the chains live; never true
+}
+
 // --- L2 read microbenchmark (roofline denominator for the table gathers) --
 // Every thread streams 16-byte loads that bypass L1 (ld.global.cg) over a
 // buffer far smaller than L2, so after the first pass every load hits L2.
@@ -866,6 +888,35 @@ int lum_session_kernel_config(lum_session* s, char* buf, size_t len) {
            o.has_somm ? (o.somm_keyed ? "lattice_keys" : "pairs") : "none",
            (long long)o.somm_records);
   return LUM_OK;
+}
+
+int lum_measure_fma2_peak(lum_ctx* ctx, double* gflops) {
+  if (bad_ptr(ctx, "ctx") || bad_ptr(gflops, "gflops")) return LUM_ERR_INVALID;
+  LUM_TRY_CUDA(cudaSetDevice(ctx->device));
+  DevBuf out;
+  LUM_TRY(out.alloc(16));
+  cudaEvent_t e0, e1;
+  LUM_TRY_CUDA(cudaEventCreate(&e0));
+  LUM_TRY_CUDA(cudaEventCreate(&e1));
+  const int threads = 256, blocks = ctx->sms * 8, iters = 2048;
+  lum_status st = LUM_OK;
+  float ms = 0.f;
+  for (int rep = 0; rep < 2 && st == LUM_OK; ++rep) {
+    cudaEventRecord(e0);
+    fma2_chain<<<blocks, threads>>>(out.as<float>(), iters, 0.999999f, 1e-7f);
+    cudaEventRecord(e1);
+    const cudaError_t e = cudaEventSynchronize(e1);
+    if (e != cudaSuccess) st = cuda_status(e, "packed FMA microbenchmark", __FILE__, __LINE__);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+  }
+  if (st == LUM_OK) {
+    cudaEventElapsedTime(&ms, e0, e1);
+    // 8 chains x 16 unrolled x 2 lanes x 2 flops per f32x2 FMA
+    *gflops = 2.0 * 2.0 * 8 * 16 * (double)iters * threads * blocks / (ms * 1e-3) / 1e9;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return st;
 }
 
 int lum_measure_l2_peak(lum_ctx* ctx, double* gbs) {
