@@ -1049,27 +1049,6 @@ static void sym2_launch_t(const OtfOperator& o, const double2* x, const double2*
 #undef LUM_SYM2_LAUNCH
 }
 
-template <int MINB>
-static void sym2v_launch_t(const OtfOperator& o, const double2* x, const double2* x2,
-                           const int* skip, const int* skip2, cudaStream_t st) {
-  const float kf = (float)o.k, s0f = (float)(o.k * o.k * o.k / (4.0 * kPi));
-  float2* s1 = o.sym_slots.as<float2>();
-  float2* s2 = s1 + (size_t)o.sym_nb * 3 * (size_t)o.n;
-#define LUM_SYM2V_LAUNCH(F, L)                                                                \
-  otf_pairs_f32_sym2v<F, L, MINB><<<o.sym_nitems, kSymRows, 0, st>>>(                         \
-      o.n, o.pos_hi.as<float4>(), o.pos_lo.as<float4>(), x, x2, kf, s0f,                     \
-      o.sym_items.as<int2>(), s1, s2, skip, skip2)
-  if (o.fast_trig && o.lofree)
-    LUM_SYM2V_LAUNCH(true, true);
-  else if (o.fast_trig)
-    LUM_SYM2V_LAUNCH(true, false);
-  else if (o.lofree)
-    LUM_SYM2V_LAUNCH(false, true);
-  else
-    LUM_SYM2V_LAUNCH(false, false);
-#undef LUM_SYM2V_LAUNCH
-}
-
 namespace {
 // Builds of the symmetric FP32 scheme the tuner chooses from: rows per
 // thread (2 or 4) x CTAs per SM (the register cap).  f32_sym is 1 + the
@@ -1100,7 +1079,6 @@ const Sym2VariantEntry kSym2Variants[] = {
     {"sym2_rows2_minb2", sym2_launch_t<2, 1>},
     {"sym2_rows2_minb1", sym2_launch_t<1, 1>},
     {"sym2_rows4_minb2", sym2_launch_t<2, 2>},
-    {"sym2_vec_minb1", sym2v_launch_t<1>},
 };
 constexpr int kNumSym2Variants = sizeof(kSym2Variants) / sizeof(kSym2Variants[0]);
 }  // namespace

@@ -362,179 +362,4 @@ otf_pairs_f32_sym2(int n, const float4* __restrict__ obs_hi, const float4* __res
                                              3 * (size_t)n, sS, sAcc, sRed);
 }
 
-// Two vectors with one row per thread: the float2 halves carry the two
-// vectors instead of two rows.  The tensor scalars of a pair are computed in
-// scalar arithmetic (the same 27 operations per unordered pair as the
-// row-packed form) and broadcast into both halves; each contraction then
-// serves both vectors in packed instructions.  Per-thread state is one row's
-// position, moments and sums, so the CTA of kSymRows threads runs without
-// the register pressure of the row-packed two-vector builds.  Shared staging
-// per source: T0 = (hx, hy, hz, lx), T1 = (ly, lz, -, -) when positions carry
-// lo parts, T2..T4 = component c as (re1, re2, im1, im2).  Both vectors are
-// always computed (a converged vector's skip flag only keeps its epilogue
-// from writing y).
-template <bool FAST, bool LOFREE, int MINB>
-__global__ void __launch_bounds__(kSymRows, MINB)
-otf_pairs_f32_sym2v(int n, const float4* __restrict__ obs_hi, const float4* __restrict__ obs_lo,
-                    const double2* __restrict__ x, const double2* __restrict__ x2, float k,
-                    float s0, const int2* __restrict__ items, float2* __restrict__ slots,
-                    float2* __restrict__ slots2, const int* __restrict__ skip,
-                    const int* __restrict__ skip2) {
-  constexpr int kWarps = kSymRows / 32;
-  if ((skip && *skip) && (skip2 && *skip2)) return;
-  __shared__ float4 sT[5][32];
-  __shared__ float2 sAcc[kWarps / 2][32][6];
-  __shared__ float2 sRed[32][6];
-  const int2 it = items[blockIdx.x];
-  const int I = it.x, J = it.y;
-  const bool diag = (I == J);
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const size_t n3 = 3 * (size_t)n;
-  const int i = I * kSymRows + tid;
-  const bool vi = i < n;
-  const float4 hi = vi ? obs_hi[i] : make_float4(2e8f, 2e8f, 2e8f, 0.f);
-  float4 lo = make_float4(0.f, 0.f, 0.f, 0.f);
-  if (!LOFREE && vi) lo = obs_lo[i];
-  float2 X[6], acc[6];  // component c: X[2c] = (re1, re2), X[2c+1] = (im1, im2)
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    const double2 a = vi ? x[3 * (size_t)i + c] : make_double2(0.0, 0.0);
-    const double2 b = vi ? x2[3 * (size_t)i + c] : make_double2(0.0, 0.0);
-    X[2 * c] = make_float2((float)a.x, (float)b.x);
-    X[2 * c + 1] = make_float2((float)a.y, (float)b.y);
-  }
-#pragma unroll
-  for (int c = 0; c < 6; ++c) acc[c] = make_float2(0.f, 0.f);
-  const float kk = k * k;
-  for (int g = 0; g < kSymRows / 32; ++g) {
-    const int jg = J * kSymRows + 32 * g;
-    if (jg >= n) break;  // CTA-uniform
-    __syncthreads();
-    if (tid < 32) {
-      const int j = jg + tid;
-      float4 h = make_float4(1e8f, 1e8f, 1e8f, 0.f), l = make_float4(0.f, 0.f, 0.f, 0.f);
-      double2 a[3] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
-      double2 b[3] = {a[0], a[0], a[0]};
-      if (j < n) {
-        h = obs_hi[j];
-        if (!LOFREE) l = obs_lo[j];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          a[c] = x[3 * (size_t)j + c];
-          b[c] = x2[3 * (size_t)j + c];
-        }
-      }
-      sT[0][tid] = make_float4(h.x, h.y, h.z, l.x);
-      sT[1][tid] = make_float4(l.y, l.z, 0.f, 0.f);
-#pragma unroll
-      for (int c = 0; c < 3; ++c)
-        sT[2 + c][tid] = make_float4((float)a[c].x, (float)b[c].x, (float)a[c].y, (float)b[c].y);
-    }
-    __syncthreads();
-    float2 sacc[6];
-#pragma unroll
-    for (int c = 0; c < 6; ++c) sacc[c] = make_float2(0.f, 0.f);
-#pragma unroll 1
-    for (int s = 0; s < 32; ++s) {
-      const int src = (lane + s) & 31;
-      const float4 T0 = sT[0][src], T2 = sT[2][src], T3 = sT[3][src], T4 = sT[4][src];
-      float dx = hi.x - T0.x, dy = hi.y - T0.y, dz = hi.z - T0.z;
-      if (!LOFREE) {
-        const float4 T1 = sT[1][src];
-        dx += lo.x - T0.w;
-        dy += lo.y - T1.x;
-        dz += lo.z - T1.y;
-      }
-      float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-      float keep = 1.f;
-      if (diag && !(jg + src > i)) {  // each unordered pair once: j > i
-        keep = 0.f;
-        if (r2 < 1e-30f) r2 = 1.f;
-      }
-      const float kr2 = r2 * kk;
-      const float u = rsqrtf(kr2);
-      const float kR = kr2 * u;
-      float sn, cs;
-      if (FAST)
-        __sincosf(kR, &sn, &cs);
-      else
-        sincosf(kR, &sn, &cs);
-      const float u2 = u * u;
-      const float q = s0 * u * keep;
-      const float pr = q * cs, pi = q * sn;
-      const float ar = 1.f - u2;
-      const float Ar = pr * ar - pi * u, Ai = fmaf(pr, u, pi * ar);
-      const float ir2 = u2 * kk;
-      const float Br = fmaf(Ar, -3.f, pr + pr) * ir2, Bi = fmaf(Ai, -3.f, pi + pi) * ir2;
-      const float2 DX = make_float2(dx, dx), DY = make_float2(dy, dy), DZ = make_float2(dz, dz);
-      const float2 AR = make_float2(Ar, Ar), AI = make_float2(Ai, Ai),
-                   NAI = make_float2(-Ai, -Ai), BR = make_float2(Br, Br),
-                   BI = make_float2(Bi, Bi), NBI = make_float2(-Bi, -Bi);
-      // row side with the source's moments, source side with the row's
-      sym_contract(DX, DY, DZ, AR, AI, NAI, BR, BI, NBI, lo2(T2), hi2(T2), lo2(T3), hi2(T3),
-                   lo2(T4), hi2(T4), acc);
-      sym_contract(DX, DY, DZ, AR, AI, NAI, BR, BI, NBI, X[0], X[1], X[2], X[3], X[4], X[5],
-                   sacc);
-      const int from = (lane + 1) & 31;
-#pragma unroll
-      for (int c = 0; c < 6; ++c) {
-        sacc[c].x = __shfl_sync(0xffffffffu, sacc[c].x, from);
-        sacc[c].y = __shfl_sync(0xffffffffu, sacc[c].y, from);
-      }
-    }
-    // fold warps w and w + kWarps / 2 (fixed order), then add the slots
-    if (warp >= kWarps / 2) {
-#pragma unroll
-      for (int c = 0; c < 6; ++c) sAcc[warp - kWarps / 2][lane][c] = sacc[c];
-    }
-    __syncthreads();
-    if (warp < kWarps / 2) {
-#pragma unroll
-      for (int c = 0; c < 6; ++c) {
-        const float2 o = sAcc[warp][lane][c];
-        sAcc[warp][lane][c] = make_float2(sacc[c].x + o.x, sacc[c].y + o.y);
-      }
-    }
-    __syncthreads();
-    if (tid < 32 * 6) {
-      const int sl = tid / 6, c = tid % 6;
-      float2 v = make_float2(0.f, 0.f);
-#pragma unroll
-      for (int w = 0; w < kWarps / 2; ++w) {
-        v.x += sAcc[w][sl][c].x;
-        v.y += sAcc[w][sl][c].y;
-      }
-      const int j = jg + sl;
-      if (diag) {
-        sRed[sl][c] = v;
-      } else if (j < n) {
-        // c = 2 * component + (0 re | 1 im); halves are the two vectors
-        float* d1 = reinterpret_cast<float*>(slots + (size_t)I * n3 + 3 * (size_t)j);
-        float* d2 = reinterpret_cast<float*>(slots2 + (size_t)I * n3 + 3 * (size_t)j);
-        d1[c] = v.x;
-        d2[c] = v.y;
-      }
-    }
-    if (diag) {  // rows 32 g .. 32 g + 31 of this item take their source-side sums
-      __syncthreads();
-      if (warp == g) {
-#pragma unroll
-        for (int c = 0; c < 6; ++c) {
-          acc[c].x += sRed[lane][c].x;
-          acc[c].y += sRed[lane][c].y;
-        }
-      }
-    }
-  }
-  if (vi) {
-    float2* d1 = slots + (size_t)J * n3 + 3 * (size_t)i;
-    float2* d2 = slots2 + (size_t)J * n3 + 3 * (size_t)i;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      d1[c] = make_float2(acc[2 * c].x, acc[2 * c + 1].x);
-      d2[c] = make_float2(acc[2 * c].y, acc[2 * c + 1].y);
-    }
-  }
-}
-
 }  // namespace lum
