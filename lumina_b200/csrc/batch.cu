@@ -30,6 +30,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstddef>
 #include <cstdlib>
 #include <cstring>
 #include <new>
@@ -60,6 +61,7 @@ struct BatchCtl {
   int m;
   int refine;
   int active;   // systems still active after the last cycle (host reads it)
+  int live_items;  // symmetric work items of those systems (host reads it with active)
 };
 
 __device__ __forceinline__ double2 zmul(double2 a, double2 b) {
@@ -191,7 +193,10 @@ __global__ void __launch_bounds__(kBT)
 k_bat_start(const int* __restrict__ sys_off, const double2* __restrict__ r,
             double2* __restrict__ V, BatchSysState* __restrict__ st,
             BatchFlags* __restrict__ flags, BatchCtl* __restrict__ ctl) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) ctl->active = 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    ctl->active = 0;
+    ctl->live_items = 0;
+  }
   const Seg sg = make_seg(sys_off);
   if (flags[sg.s].frozen) return;  // cluster-uniform
   BatchSysState& S = st[sg.s];
@@ -403,7 +408,7 @@ __global__ void __launch_bounds__(kBT)
 k_bat_residual(const int* __restrict__ sys_off, const double2* __restrict__ b,
                const double2* __restrict__ ax, double2* __restrict__ r,
                BatchSysState* __restrict__ st, BatchFlags* __restrict__ flags,
-               BatchCtl* __restrict__ ctl) {
+               BatchCtl* __restrict__ ctl, const int* __restrict__ sys_nb) {
   __shared__ ClusterSum cs;
   const Seg sg = make_seg(sys_off);
   const BatchFlags f = flags[sg.s];
@@ -439,6 +444,10 @@ k_bat_residual(const int* __restrict__ sys_off, const double2* __restrict__ b,
       F.frozen = 1;
     } else {
       atomicAdd(&ctl->active, 1);
+      if (sys_nb) {
+        const int nb = sys_nb[sg.s];
+        atomicAdd(&ctl->live_items, nb * (nb + 1) / 2);
+      }
     }
   }
   cg::this_cluster().sync();
@@ -485,13 +494,18 @@ struct lum_batch {
   // solver workspace
   int m = 0;
   DevBuf V, w, r, tmp, xs, bs, state, flags, ctl;
-  int* h_active = nullptr;
+  int* h_active = nullptr;  // [0] active systems, [1] their symmetric work items
   BatchSysState* h_state = nullptr;
   BatchFlags* h_flags = nullptr;
-  cudaGraphExec_t graph[2] = {nullptr, nullptr};
-  int graph_m[2] = {0, 0};
-  uint64_t graph_launches[2] = {0, 0};
+  // cycle graphs: FP64, FP32 on the split work list, FP32 on the symmetric one
+  cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
+  int graph_m[3] = {0, 0, 0};
+  uint64_t graph_launches[3] = {0, 0, 0};
   int use_graph = 1;
+  // A cycle of FP32 products takes the symmetric build g.sym32 while the
+  // active systems hold at least sym_min_items symmetric items; below that
+  // the split list, whose finer items keep the grid busy on a few systems.
+  int sym_min_items = 0;
   // Right-hand-side batch (lum_batch_create_rhs): K vectors of one session's
   // operator, applied through that session instead of the pair work list.
   lum_session* src = nullptr;
@@ -562,7 +576,8 @@ struct RunResidual {
     return launch_cluster(k_bat_residual<E>, B->K, B->cl, B->stream, B->d_off.as<const int>(),
                           B->bs.as<const double2>(), B->tmp.as<const double2>(),
                           B->r.as<double2>(), B->state.as<BatchSysState>(),
-                          B->flags.as<BatchFlags>(), B->ctl.as<BatchCtl>());
+                          B->flags.as<BatchFlags>(), B->ctl.as<BatchCtl>(),
+                          B->d_nb.as<const int>());
   }
 };
 
@@ -638,7 +653,7 @@ lum_status batch_workspace(lum_batch* B, int m) {
     LUM_TRY(B->flags.alloc(sizeof(BatchFlags) * (size_t)B->K));
     LUM_TRY(B->ctl.alloc(sizeof(BatchCtl)));
     LUM_TRY_CUDA(cudaMemsetAsync(B->flags.p, 0, B->flags.bytes, B->stream));
-    if (!B->h_active) LUM_TRY_CUDA(cudaMallocHost((void**)&B->h_active, sizeof(int)));
+    if (!B->h_active) LUM_TRY_CUDA(cudaMallocHost((void**)&B->h_active, 2 * sizeof(int)));
     if (!B->h_state)
       LUM_TRY_CUDA(cudaMallocHost((void**)&B->h_state, sizeof(BatchSysState) * (size_t)B->K));
     if (!B->h_flags)
@@ -672,36 +687,42 @@ lum_status rhs_apply(lum_batch* B, int prec, const double2* x, double2* y) {
   return LUM_OK;
 }
 
-// One restart cycle for all systems (the body that is captured as a graph).
-lum_status batch_cycle(lum_batch* B, int mode) {
+// One restart cycle for all systems (the body that is captured as a graph);
+// sym != 0 runs its FP32 products on symmetric build sym.
+lum_status batch_cycle(lum_batch* B, int mode, int sym) {
   const int prec = (mode == LUM_SOLVE_FP32_REFINE) ? LUM_FP32 : LUM_FP64;
   const size_t len = 3 * (size_t)B->N;
   BatchQueue& qa = (prec == LUM_FP32) ? B->q32 : B->q64;
+  BatchGeom g = B->g;
+  g.sym32 = sym;
   const BatchFlags* fl = B->flags.as<BatchFlags>();
   LUM_TRY(dispatch_ept<RunStart>(B->ept, B));
   for (int j = 0; j < B->m; ++j) {
     if (B->src)
       LUM_TRY(rhs_apply(B, prec, B->V.as<double2>() + (size_t)j * len, B->w.as<double2>()));
     else
-      LUM_TRY(batch_apply(B->g, prec, B->V.as<double2>() + (size_t)j * len,
-                          B->w.as<double2>(), B->part.p, qa, fl, 1, B->stream));
+      LUM_TRY(batch_apply(g, prec, B->V.as<double2>() + (size_t)j * len, B->w.as<double2>(),
+                          B->part.p, qa, fl, 1, B->stream));
     LUM_TRY(dispatch_ept<RunArnoldi>(B->ept, B, j));
   }
   LUM_TRY(dispatch_ept<RunUpdate>(B->ept, B));
   if (B->src)
     LUM_TRY(rhs_apply(B, LUM_FP64, B->xs.as<double2>(), B->tmp.as<double2>()));
   else
-    LUM_TRY(batch_apply(B->g, LUM_FP64, B->xs.as<double2>(), B->tmp.as<double2>(), B->part.p,
+    LUM_TRY(batch_apply(g, LUM_FP64, B->xs.as<double2>(), B->tmp.as<double2>(), B->part.p,
                         B->q64, fl, 2, B->stream));
   LUM_TRY(dispatch_ept<RunResidual>(B->ept, B));
-  LUM_TRY_CUDA(cudaMemcpyAsync(B->h_active, &B->ctl.as<BatchCtl>()->active, sizeof(int),
+  static_assert(offsetof(BatchCtl, live_items) == offsetof(BatchCtl, active) + sizeof(int),
+                "active and live_items are read together");
+  LUM_TRY_CUDA(cudaMemcpyAsync(B->h_active, &B->ctl.as<BatchCtl>()->active, 2 * sizeof(int),
                                cudaMemcpyDeviceToHost, B->stream));
   return LUM_OK;
 }
 
-lum_status batch_run_cycle(lum_batch* B, int mode) {
-  const int gi = (mode == LUM_SOLVE_FP32_REFINE) ? 1 : 0;
-  if (!B->use_graph) return batch_cycle(B, mode);
+// Captures and instantiates the cycle graph of (mode, sym) unless it exists
+// for the current restart length.
+lum_status batch_graph(lum_batch* B, int mode, int sym) {
+  const int gi = (mode == LUM_SOLVE_FP32_REFINE) ? (sym ? 2 : 1) : 0;
   if (!B->graph[gi] || B->graph_m[gi] != B->m) {
     if (B->graph[gi]) {
       cudaGraphExecDestroy(B->graph[gi]);
@@ -710,7 +731,7 @@ lum_status batch_run_cycle(lum_batch* B, int mode) {
     cudaGraph_t gr = nullptr;
     LUM_TRY_CUDA(cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal));
     const uint64_t l0 = g_launches.load();
-    lum_status s = batch_cycle(B, mode);
+    lum_status s = batch_cycle(B, mode, sym);
     cudaError_t e = cudaStreamEndCapture(B->stream, &gr);
     if (s != LUM_OK) {
       if (gr) cudaGraphDestroy(gr);
@@ -728,6 +749,13 @@ lum_status batch_run_cycle(lum_batch* B, int mode) {
     }
     B->graph_m[gi] = B->m;
   }
+  return LUM_OK;
+}
+
+lum_status batch_run_cycle(lum_batch* B, int mode, int sym) {
+  const int gi = (mode == LUM_SOLVE_FP32_REFINE) ? (sym ? 2 : 1) : 0;
+  if (!B->use_graph) return batch_cycle(B, mode, sym);
+  LUM_TRY(batch_graph(B, mode, sym));
   LUM_TRY_CUDA(cudaGraphLaunch(B->graph[gi], B->stream));
   g_launches.fetch_add(B->graph_launches[gi]);
   return LUM_OK;
@@ -923,6 +951,8 @@ int lum_batch_create(lum_ctx* ctx, int n_systems, const int* sys_dipoles, const 
                     3 * (size_t)N;
   LUM_B_TRY(B->part.alloc(pb));
   LUM_B_TRY(batch_choose_scheme(B, st));
+  B->sym_min_items = 4 * sms * sym_occ;  // four items per CTA slot of the persistent grid
+  if (const char* e = std::getenv("LUMINA_BATCH_SYM_MIN_ITEMS")) B->sym_min_items = std::atoi(e);
 #undef LUM_B_UP
 #undef LUM_B_TRY
   ce = cudaStreamSynchronize(st);
@@ -1046,7 +1076,9 @@ int lum_batch_kernel_config(lum_batch* B, char* buf, size_t len) {
            g.fast);
   if (g.sym32) {
     const size_t used = strlen(buf);
-    if (used + 1 < len) snprintf(buf + used, len - used, " sym_variant=%s", batch_sym_name(g.sym32));
+    if (used + 1 < len)
+      snprintf(buf + used, len - used, " sym_variant=%s sym_min_items=%d split_items32=%d",
+               batch_sym_name(g.sym32), B->sym_min_items, B->q32.nitems);
   }
   return LUM_OK;
 }
@@ -1123,11 +1155,27 @@ int lum_batch_solve_device(lum_batch* B, const void* b_dev, void* x_dev, double 
   // result unwritten: the cycle's status is read after every cycle
   const bool tensor = B->src && B->src->kind == 1 && B->src->cached.precision == LUM_FP32 &&
                       mode == LUM_SOLVE_FP32_REFINE;
+  // symmetric items of the systems still active (all of them at the start)
+  long live = 0;
+  if (!B->src)
+    for (int s = 0; s < B->K; ++s) {
+      const long nb = (B->off[s + 1] - B->off[s] + kBatchSymRows - 1) / kBatchSymRows;
+      live += nb * (nb + 1) / 2;
+    }
+  if (B->use_graph && mode == LUM_SOLVE_FP32_REFINE && B->g.sym32) {
+    // both FP32 cycle graphs before the first cycle: none is captured mid-solve
+    LUM_TRY(batch_graph(B, mode, B->g.sym32));
+    LUM_TRY(batch_graph(B, mode, 0));
+  }
   for (long cyc = 0; cyc < max_cycles; ++cyc) {
-    LUM_TRY(batch_run_cycle(B, mode));
+    const int sym = (mode == LUM_SOLVE_FP32_REFINE && B->g.sym32 && live >= B->sym_min_items)
+                        ? B->g.sym32
+                        : 0;
+    LUM_TRY(batch_run_cycle(B, mode, sym));
     LUM_TRY_CUDA(cudaStreamSynchronize(st));
     if (tensor) LUM_TRY(lum::cgemm_status(B->src->cached, st));
-    if (*B->h_active == 0) break;
+    if (B->h_active[0] == 0) break;
+    live = B->h_active[1];
   }
   LUM_TRY_CUDA(cudaMemcpyAsync(x_dev, B->xs.p, bytes, cudaMemcpyDeviceToDevice, st));
   LUM_TRY_CUDA(cudaMemcpyAsync(B->h_state, B->state.p, sizeof(BatchSysState) * (size_t)B->K,

@@ -377,6 +377,9 @@ lum_status batch_apply(const BatchGeom& g, int precision, const double2* x, doub
                        void* partial, BatchQueue& q, const BatchFlags* flags, int skip_mode,
                        cudaStream_t st);                                             // otf.cu
 int batch_occupancy(const BatchGeom& g, int precision);                              // otf.cu
+// Rows (and sources) of a superblock of the symmetric scheme; a system of n
+// dipoles has ceil(n / kBatchSymRows) superblocks and nb (nb + 1) / 2 items.
+constexpr int kBatchSymRows = 512;
 lum_status batch_queue_sym(const std::vector<int>& off, int slots, BatchQueue& q,
                            std::vector<int>& nb, cudaStream_t st);                   // otf.cu
 int batch_sym_variants();                                                            // otf.cu

@@ -1009,12 +1009,13 @@ lum_status OtfOperator::sym_prepare(cudaStream_t st) {
   return LUM_OK;
 }
 
-template <int MINB, int RP, int UNR = 1>
+template <int MINB, int RP, int UNR = 1, bool PIPE = false>
 static void sym_launch_t(const OtfOperator& o, const double2* x, const int* skip,
                          cudaStream_t st) {
   const float kf = (float)o.k, s0f = (float)(o.k * o.k * o.k / (4.0 * kPi));
 #define LUM_SYM_LAUNCH(F, L)                                                                  \
-  otf_pairs_f32_sym<F, L, MINB, RP, UNR><<<o.sym_nitems, SymShape<RP>::kThreads, 0, st>>>(    \
+  otf_pairs_f32_sym<F, L, MINB, RP, UNR, PIPE>                                                \
+      <<<o.sym_nitems, SymShape<RP>::kThreads, 0, st>>>(                                      \
       o.n, o.pos_hi.as<float4>(), o.pos_lo.as<float4>(), x, kf, s0f, o.sym_items.as<int2>(), \
       o.sym_slots.as<float2>(), skip)
   if (o.fast_trig && o.lofree)
@@ -1066,6 +1067,8 @@ const SymVariantEntry kSymVariants[] = {
     {"sym_rows4_minb3_unroll2", sym_launch_t<3, 2, 2>},
     {"sym_rows8_minb4", sym_launch_t<4, 4>},
     {"sym_rows8_minb5", sym_launch_t<5, 4>},
+    {"sym_rows4_minb3_pipe", sym_launch_t<3, 2, 1, true>},
+    {"sym_rows2_minb2_pipe", sym_launch_t<2, 1, 1, true>},
 };
 constexpr int kNumSymVariants = sizeof(kSymVariants) / sizeof(kSymVariants[0]);
 
@@ -1112,11 +1115,13 @@ lum_status OtfOperator::tune_f32(cudaStream_t st) {
   f32_sym = 0;
   nsplit32 = nsplit_v[0];
   const bool isolated = !has_lattice && !has_substrate;
-  // LUMINA_F32_SYM=v (1..4) forces symmetric build v on isolated systems
-  // (no lattice, no substrate image); =0 excludes the symmetric scheme.
+  // LUMINA_F32_SYM=v (1..kNumSymVariants) forces symmetric build v on
+  // isolated systems (no lattice, no substrate image); =0 excludes the
+  // symmetric scheme.
   const char* sym_env = std::getenv("LUMINA_F32_SYM");
-  if (isolated && sym_env && sym_env[0] >= '1' && sym_env[0] <= '9') {
-    f32_sym = std::min(sym_env[0] - '0', kNumSymVariants);
+  const int sym_forced = sym_env ? std::atoi(sym_env) : 0;
+  if (isolated && sym_forced >= 1) {
+    f32_sym = std::min(sym_forced, kNumSymVariants);
     return sym_prepare(st);
   }
   const bool sym_allowed = isolated && !(sym_env && sym_env[0] == '0');
@@ -1849,6 +1854,8 @@ const char* batch_sym_name(int v) {
 int batch_sym_occupancy(const BatchGeom& g, int v) {
   return kBatchSym[std::min(std::max(v, 1), kNumBatchSym) - 1].occupancy(g);
 }
+
+static_assert(kSymRows == kBatchSymRows, "one superblock size for the batch and its kernels");
 
 // Work list of the symmetric scheme: every superblock pair (I <= J) of every
 // system, ordered by decreasing cost (diagonal pairs count half).

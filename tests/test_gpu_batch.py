@@ -175,11 +175,13 @@ def test_batch_symmetric_scheme_matches_oracle(backend, rng, monkeypatch, varian
     diagonal blocks are crossed; every system against the oracle, and the
     FP32+refine solve against the FP64 one."""
     monkeypatch.setenv("LUMINA_BATCH_SYM", variant)
+    monkeypatch.setenv("LUMINA_BATCH_SYM_MIN_ITEMS", "0")  # every FP32 cycle symmetric
     w = small_batch(count=3, seed=7, n_range=(200, 1400))
     systems, specs = batch_inputs(w)
     with backend.create_batch(specs) as B:
         cfg = B.kernel_config()
         assert cfg["fp32_scheme"] == "symmetric" and cfg["sym32"] == int(variant)
+        assert cfg["sym_min_items"] == 0
         x = rand_vec(rng, B.dim)
         y32 = B.split(B.matvec(x, "fp32"))
         xs = B.split(x)
@@ -193,3 +195,36 @@ def test_batch_symmetric_scheme_matches_oracle(backend, rng, monkeypatch, varian
             c32 = lb.cross_sections(p, inv, B.split(x32)[s], k, inc)[0]
             c64 = lb.cross_sections(p, inv, B.split(x64)[s], k, inc)[0]
             assert abs(c32 - c64) <= 1e-6 * abs(c64), (variant, s)
+
+
+def test_batch_scheme_switch_mid_solve(backend, monkeypatch):
+    """A cycle runs the symmetric build while the active systems hold at
+    least LUMINA_BATCH_SYM_MIN_ITEMS symmetric items, the split list below
+    that.  With the threshold at the batch's full item count the first cycles
+    are symmetric and the rest, once a system has converged, split: the
+    FP32+refine solve still matches the FP64 one and the solves under either
+    scheme alone (tolerance 1e-8, the clusters benchmark's; these Drude
+    clusters take thousands of iterations)."""
+    monkeypatch.setenv("LUMINA_BATCH_SYM", "2")
+    w = small_batch(count=4, seed=11, n_range=(300, 1500))
+    systems, specs = batch_inputs(w)
+    total = sum(((p.shape[0] + 511) // 512) * ((p.shape[0] + 511) // 512 + 1) // 2
+                for p, _, _, _ in specs)
+    b = np.concatenate([lb.incident_field(p, k, inc) for p, _, k, _, inc in systems])
+    cext = {}
+    for label, min_items in (("hybrid", total), ("sym", 0), ("split", 10 ** 9)):
+        monkeypatch.setenv("LUMINA_BATCH_SYM_MIN_ITEMS", str(min_items))
+        with backend.create_batch(specs) as B:
+            assert B.kernel_config()["sym_min_items"] == min_items
+            x32, i32 = B.solve(b, 1e-8, 20000, 30, "fp32_refine")
+            x64, _ = B.solve(b, 1e-8, 20000, 30, "fp64")
+            cext[label] = []
+            for s, ((p, inv, k, cell), (_, _, _, _, inc)) in enumerate(zip(specs, systems)):
+                c32 = lb.cross_sections(p, inv, B.split(x32)[s], k, inc)[0]
+                c64 = lb.cross_sections(p, inv, B.split(x64)[s], k, inc)[0]
+                assert i32[s]["converged"] == 1, (label, s)
+                assert abs(c32 - c64) <= 1e-6 * abs(c64), (label, s)
+                cext[label].append(c32)
+    for s in range(len(specs)):
+        for label in ("hybrid", "sym"):
+            assert abs(cext[label][s] - cext["split"][s]) <= 1e-6 * abs(cext["split"][s])
