@@ -1009,13 +1009,12 @@ lum_status OtfOperator::sym_prepare(cudaStream_t st) {
   return LUM_OK;
 }
 
-template <int MINB, int RP, int UNR = 1, bool PIPE = false>
+template <int MINB, int RP, int UNR = 1>
 static void sym_launch_t(const OtfOperator& o, const double2* x, const int* skip,
                          cudaStream_t st) {
   const float kf = (float)o.k, s0f = (float)(o.k * o.k * o.k / (4.0 * kPi));
 #define LUM_SYM_LAUNCH(F, L)                                                                  \
-  otf_pairs_f32_sym<F, L, MINB, RP, UNR, PIPE>                                                \
-      <<<o.sym_nitems, SymShape<RP>::kThreads, 0, st>>>(                                      \
+  otf_pairs_f32_sym<F, L, MINB, RP, UNR><<<o.sym_nitems, SymShape<RP>::kThreads, 0, st>>>(    \
       o.n, o.pos_hi.as<float4>(), o.pos_lo.as<float4>(), x, kf, s0f, o.sym_items.as<int2>(), \
       o.sym_slots.as<float2>(), skip)
   if (o.fast_trig && o.lofree)
@@ -1067,8 +1066,6 @@ const SymVariantEntry kSymVariants[] = {
     {"sym_rows4_minb3_unroll2", sym_launch_t<3, 2, 2>},
     {"sym_rows8_minb4", sym_launch_t<4, 4>},
     {"sym_rows8_minb5", sym_launch_t<5, 4>},
-    {"sym_rows4_minb3_pipe", sym_launch_t<3, 2, 1, true>},
-    {"sym_rows2_minb2_pipe", sym_launch_t<2, 1, 1, true>},
 };
 constexpr int kNumSymVariants = sizeof(kSymVariants) / sizeof(kSymVariants[0]);
 

@@ -23,11 +23,6 @@
 // loads and shuffles per pair and gives each step two independent tensor
 // evaluations to interleave, at the cost of registers; UNR = 2 unrolls the
 // step loop so that one step's shuffles overlap the next step's tensor.
-// PIPE = true software-pipelines the steps (one vector): step s evaluates the
-// tensor scalars against the source of step s + 1 while it contracts those
-// of step s, so the serial chain through rsqrt and sin/cos of one source
-// overlaps the FMA work of the previous one.  Two register sets of scalars
-// alternate between the steps (no copies).
 //
 // NV = 2 applies the operator to two vectors at once (forward + adjoint,
 // two polarisations): the tensor scalars are evaluated once per unordered
@@ -120,78 +115,13 @@ __device__ __forceinline__ void sym_contract(float2 dx, float2 dy, float2 dz, fl
   acc[5] = fma2(ti, dz, fma2(Ar, v2i, fma2(Ai, v2r, acc[5])));
 }
 
-// Tensor scalars of a packed row pair against one source (the pipelined
-// steps keep two sets; -Ai and -Bi are formed when they are contracted).
-struct SymTensor {
-  float2 dx, dy, dz, Ar, Ai, Br, Bi;
-};
-
-// The scalars of the RP row pairs against staged source src (dipole j), and
-// the two components of its moment that sit in the same staged words.
-template <bool FAST, bool LOFREE, int RP>
-__device__ __forceinline__ void sym_tensors(
-    const float2 (&OX)[RP], const float2 (&OY)[RP], const float2 (&OZ)[RP],
-    const float2 (&LX)[RP], const float2 (&LY)[RP], const float2 (&LZ)[RP], float4 (*sS)[32],
-    int src, bool diag, int j, const int (&ia)[RP], const int (&ib)[RP], float2 kk2,
-    float2 s02, SymTensor (&T)[RP], float2& x0r, float2& x2i) {
-  const float4 S0 = sS[0][src], S1 = sS[1][src], S4 = sS[4][src];
-  float4 S5 = make_float4(0.f, 0.f, 0.f, 0.f);
-  if (!LOFREE) S5 = sS[5][src];
-  x0r = hi2(S1);
-  x2i = lo2(S4);
-#pragma unroll
-  for (int p = 0; p < RP; ++p) {
-    float2 nAi, nBi;  // not kept
-    sym_pair_tensor<FAST, LOFREE>(OX[p], OY[p], OZ[p], LX[p], LY[p], LZ[p], S0, S1, S4, S5,
-                                  diag, j, ia[p], ib[p], kk2, s02, T[p].dx, T[p].dy, T[p].dz,
-                                  T[p].Ar, T[p].Ai, nAi, T[p].Br, T[p].Bi, nBi);
-  }
-}
-
-// One pipelined step s: contracts the scalars Tc of source (lane + s) mod 32
-// on both sides and, when NEXT, evaluates those of source (lane + s + 1)
-// mod 32 into Tn; then passes the source-side sums on.
-template <bool FAST, bool LOFREE, int RP, bool NEXT>
-__device__ __forceinline__ void sym_step_pipe(
-    const float2 (&OX)[RP], const float2 (&OY)[RP], const float2 (&OZ)[RP],
-    const float2 (&LX)[RP], const float2 (&LY)[RP], const float2 (&LZ)[RP],
-    const float2 (&X)[RP][1][6], float2 (&acc)[RP][1][6], float2 (&sacc)[1][6],
-    float4 (*sS)[32], int s, int lane, bool diag, int jg, const int (&ia)[RP],
-    const int (&ib)[RP], float2 kk2, float2 s02, const SymTensor (&Tc)[RP], float2 cx0r,
-    float2 cx2i, SymTensor (&Tn)[RP], float2& nx0r, float2& nx2i) {
-  const float2 m1 = make_float2(-1.0f, -1.0f);
-  const int src = (lane + s) & 31;
-  if constexpr (NEXT) {
-    const int srcn = (lane + s + 1) & 31;
-    sym_tensors<FAST, LOFREE, RP>(OX, OY, OZ, LX, LY, LZ, sS, srcn, diag, jg + srcn, ia, ib,
-                                  kk2, s02, Tn, nx0r, nx2i);
-  }
-  const float4 S2 = sS[2][src], S3 = sS[3][src];
-  const float2 x0i = lo2(S2), x1r = hi2(S2), x1i = lo2(S3), x2r = hi2(S3);
-#pragma unroll
-  for (int p = 0; p < RP; ++p) {
-    const SymTensor& t = Tc[p];
-    const float2 nAi = mul2(t.Ai, m1), nBi = mul2(t.Bi, m1);
-    sym_contract(t.dx, t.dy, t.dz, t.Ar, t.Ai, nAi, t.Br, t.Bi, nBi, cx0r, x0i, x1r, x1i, x2r,
-                 cx2i, acc[p][0]);
-    sym_contract(t.dx, t.dy, t.dz, t.Ar, t.Ai, nAi, t.Br, t.Bi, nBi, X[p][0][0], X[p][0][1],
-                 X[p][0][2], X[p][0][3], X[p][0][4], X[p][0][5], sacc[0]);
-  }
-  const int from = (lane + 1) & 31;
-#pragma unroll
-  for (int c = 0; c < 6; ++c) {
-    sacc[0][c].x = __shfl_sync(0xffffffffu, sacc[0][c].x, from);
-    sacc[0][c].y = __shfl_sync(0xffffffffu, sacc[0][c].y, from);
-  }
-}
-
 // The work of one superblock pair for NV vectors.  Slot S of a vector starts
 // at slots + S * slot_stride (3n for one system; 3N for a batch, whose
 // systems share the slot layout of the global dipole range).  Shared memory
 // comes from the caller: sS [6 + 3 (NV - 1)][32] staged sources, sAcc
 // [warps][32][6 NV] per-warp source sums, sRed [32][6 NV] the diagonal
 // hand-off.
-template <bool FAST, bool LOFREE, int RP, int NV, int UNR = 1, bool PIPE = false>
+template <bool FAST, bool LOFREE, int RP, int NV, int UNR = 1>
 __device__ __forceinline__ void sym_superblock_pair(
     int n, const float4* __restrict__ obs_hi, const float4* __restrict__ obs_lo,
     const double2* __restrict__ xa_v, const double2* __restrict__ xb_v, float k, float s0,
@@ -199,7 +129,6 @@ __device__ __forceinline__ void sym_superblock_pair(
     float4 (*sS)[32], float2* sAcc, float* sRed) {
   constexpr int kThreads = SymShape<RP>::kThreads, kWarps = SymShape<RP>::kWarps;
   constexpr int W = 6 * NV;  // floats of source-side sum per source
-  static_assert(!PIPE || NV == 1, "the pipelined steps take one vector");
   const double2* xv[2] = {xa_v, xb_v};
   float2* sl_v[2] = {slots_a, slots_b};
   const bool diag = (I == J);
@@ -286,27 +215,6 @@ __device__ __forceinline__ void sym_superblock_pair(
     for (int v = 0; v < NV; ++v)
 #pragma unroll
       for (int c = 0; c < 6; ++c) sacc[v][c] = make_float2(0.f, 0.f);
-    if constexpr (PIPE) {
-      SymTensor TA[RP], TB[RP];
-      float2 ax0r, ax2i, bx0r, bx2i;
-      sym_tensors<FAST, LOFREE, RP>(OX, OY, OZ, LX, LY, LZ, sS, lane, diag, jg + lane, ia, ib,
-                                    kk2, s02, TA, ax0r, ax2i);
-#pragma unroll 1
-      for (int s = 0; s < 30; s += 2) {
-        sym_step_pipe<FAST, LOFREE, RP, true>(OX, OY, OZ, LX, LY, LZ, X, acc, sacc, sS, s, lane,
-                                              diag, jg, ia, ib, kk2, s02, TA, ax0r, ax2i, TB,
-                                              bx0r, bx2i);
-        sym_step_pipe<FAST, LOFREE, RP, true>(OX, OY, OZ, LX, LY, LZ, X, acc, sacc, sS, s + 1,
-                                              lane, diag, jg, ia, ib, kk2, s02, TB, bx0r, bx2i,
-                                              TA, ax0r, ax2i);
-      }
-      sym_step_pipe<FAST, LOFREE, RP, true>(OX, OY, OZ, LX, LY, LZ, X, acc, sacc, sS, 30, lane,
-                                            diag, jg, ia, ib, kk2, s02, TA, ax0r, ax2i, TB, bx0r,
-                                            bx2i);
-      sym_step_pipe<FAST, LOFREE, RP, false>(OX, OY, OZ, LX, LY, LZ, X, acc, sacc, sS, 31, lane,
-                                             diag, jg, ia, ib, kk2, s02, TB, bx0r, bx2i, TA,
-                                             ax0r, ax2i);
-    } else {
 #pragma unroll UNR
     for (int s = 0; s < 32; ++s) {
       const int src = (lane + s) & 31;
@@ -350,7 +258,6 @@ __device__ __forceinline__ void sym_superblock_pair(
           sacc[v][c].x = __shfl_sync(0xffffffffu, sacc[v][c].x, from);
           sacc[v][c].y = __shfl_sync(0xffffffffu, sacc[v][c].y, from);
         }
-    }
     }
     // lane l now holds source l's sums over the warp's rows (halves a / b)
 #pragma unroll
@@ -415,7 +322,7 @@ __device__ __forceinline__ void sym_superblock_pair(
     }
 }
 
-template <bool FAST, bool LOFREE, int MINB, int RP, int UNR = 1, bool PIPE = false>
+template <bool FAST, bool LOFREE, int MINB, int RP, int UNR = 1>
 __global__ void __launch_bounds__(SymShape<RP>::kThreads, MINB)
 otf_pairs_f32_sym(int n, const float4* __restrict__ obs_hi, const float4* __restrict__ obs_lo,
                   const double2* __restrict__ x, float k, float s0,
@@ -426,9 +333,9 @@ otf_pairs_f32_sym(int n, const float4* __restrict__ obs_hi, const float4* __rest
   __shared__ float2 sAcc[SymShape<RP>::kWarps * 32 * 6];
   __shared__ float sRed[32 * 6];
   const int2 it = items[blockIdx.x];
-  sym_superblock_pair<FAST, LOFREE, RP, 1, UNR, PIPE>(n, obs_hi, obs_lo, x, nullptr, k, s0,
-                                                      it.x, it.y, slots, nullptr, 3 * (size_t)n,
-                                                      sS, sAcc, sRed);
+  sym_superblock_pair<FAST, LOFREE, RP, 1, UNR>(n, obs_hi, obs_lo, x, nullptr, k, s0, it.x,
+                                                it.y, slots, nullptr, 3 * (size_t)n, sS, sAcc,
+                                                sRed);
 }
 
 // Two vectors (see NV above).  A vector whose skip flag is set is left out;
