@@ -1066,6 +1066,9 @@ const SymVariantEntry kSymVariants[] = {
     {"sym_rows4_minb3_unroll2", sym_launch_t<3, 2, 2>},
     {"sym_rows8_minb4", sym_launch_t<4, 4>},
     {"sym_rows8_minb5", sym_launch_t<5, 4>},
+    {"sym_rows4_minb4_unroll2", sym_launch_t<4, 2, 2>},
+    {"sym_rows4_minb3_unroll4", sym_launch_t<3, 2, 4>},
+    {"sym_rows8_minb4_unroll2", sym_launch_t<4, 4, 2>},
 };
 constexpr int kNumSymVariants = sizeof(kSymVariants) / sizeof(kSymVariants[0]);
 

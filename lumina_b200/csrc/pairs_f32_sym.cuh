@@ -115,14 +115,14 @@ __device__ __forceinline__ void sym_contract(float2 dx, float2 dy, float2 dz, fl
   acc[5] = fma2(ti, dz, fma2(Ar, v2i, fma2(Ai, v2r, acc[5])));
 }
 
-// The work of one superblock pair for NV vectors.  Slot S of a vector starts
-// at slots + S * slot_stride (3n for one system; 3N for a batch, whose
-// systems share the slot layout of the global dipole range).  Shared memory
-// comes from the caller: sS [6 + 3 (NV - 1)][32] staged sources, sAcc
-// [warps][32][6 NV] per-warp source sums, sRed [32][6 NV] the diagonal
-// hand-off.
-template <bool FAST, bool LOFREE, int RP, int NV, int UNR = 1>
-__device__ __forceinline__ void sym_superblock_pair(
+// The work of one superblock pair for NV vectors (DIAG: the item I == J).
+// Slot S of a vector starts at slots + S * slot_stride (3n for one system; 3N
+// for a batch, whose systems share the slot layout of the global dipole
+// range).  Shared memory comes from the caller: sS [6 + 3 (NV - 1)][32]
+// staged sources, sAcc [warps][32][6 NV] per-warp source sums, sRed
+// [32][6 NV] the diagonal hand-off.
+template <bool FAST, bool LOFREE, int RP, int NV, int UNR, bool DIAG>
+__device__ __forceinline__ void sym_superblock_pair_t(
     int n, const float4* __restrict__ obs_hi, const float4* __restrict__ obs_lo,
     const double2* __restrict__ xa_v, const double2* __restrict__ xb_v, float k, float s0,
     int I, int J, float2* __restrict__ slots_a, float2* __restrict__ slots_b, size_t slot_stride,
@@ -131,7 +131,7 @@ __device__ __forceinline__ void sym_superblock_pair(
   constexpr int W = 6 * NV;  // floats of source-side sum per source
   const double2* xv[2] = {xa_v, xb_v};
   float2* sl_v[2] = {slots_a, slots_b};
-  const bool diag = (I == J);
+  constexpr bool diag = DIAG;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   // rows of this thread: pair p holds a = lane, b = lane + 32 of its 64;
@@ -320,6 +320,25 @@ __device__ __forceinline__ void sym_superblock_pair(
         for (int c = 0; c < 3; ++c) dst[c] = make_float2(acc[p][v][2 * c].y, acc[p][v][2 * c + 1].y);
       }
     }
+}
+
+// The diagonal items (one per superblock) and the off-diagonal ones are
+// separate instantiations, so the masking of the diagonal stays out of the
+// off-diagonal step loop.
+template <bool FAST, bool LOFREE, int RP, int NV, int UNR = 1>
+__device__ __forceinline__ void sym_superblock_pair(
+    int n, const float4* __restrict__ obs_hi, const float4* __restrict__ obs_lo,
+    const double2* __restrict__ xa_v, const double2* __restrict__ xb_v, float k, float s0,
+    int I, int J, float2* __restrict__ slots_a, float2* __restrict__ slots_b, size_t slot_stride,
+    float4 (*sS)[32], float2* sAcc, float* sRed) {
+  if (I == J)
+    sym_superblock_pair_t<FAST, LOFREE, RP, NV, UNR, true>(n, obs_hi, obs_lo, xa_v, xb_v, k, s0,
+                                                           I, J, slots_a, slots_b, slot_stride,
+                                                           sS, sAcc, sRed);
+  else
+    sym_superblock_pair_t<FAST, LOFREE, RP, NV, UNR, false>(n, obs_hi, obs_lo, xa_v, xb_v, k, s0,
+                                                            I, J, slots_a, slots_b, slot_stride,
+                                                            sS, sAcc, sRed);
 }
 
 template <bool FAST, bool LOFREE, int MINB, int RP, int UNR = 1>
