@@ -27,8 +27,8 @@ namespace lum {
 
 constexpr int kSym64Threads = kSymRows;  // one row per thread
 
-template <int NV>
-__device__ __forceinline__ void sym64_superblock_pair(
+template <int NV, bool DIAG>
+__device__ __forceinline__ void sym64_superblock_pair_t(
     int n, const double4* __restrict__ pos, const double2* __restrict__ xa_v,
     const double2* __restrict__ xb_v, double k, double inv_k, double s0, int I, int J,
     double2* __restrict__ slots_a, double2* __restrict__ slots_b, double4* sP,
@@ -37,7 +37,7 @@ __device__ __forceinline__ void sym64_superblock_pair(
   constexpr int kHalf = kWarps / 2;
   const double2* xv[2] = {xa_v, xb_v};
   double2* sl_v[2] = {slots_a, slots_b};
-  const bool diag = (I == J);
+  constexpr bool diag = DIAG;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const size_t n3 = 3 * (size_t)n;
 
@@ -186,6 +186,22 @@ __device__ __forceinline__ void sym64_superblock_pair(
       for (int c = 0; c < 3; ++c) dst[c] = make_double2(acc[v][2 * c], acc[v][2 * c + 1]);
     }
   }
+}
+
+// Diagonal and off-diagonal items as separate instantiations: the masking
+// of the diagonal stays out of the off-diagonal step loop.
+template <int NV>
+__device__ __forceinline__ void sym64_superblock_pair(
+    int n, const double4* __restrict__ pos, const double2* __restrict__ xa_v,
+    const double2* __restrict__ xb_v, double k, double inv_k, double s0, int I, int J,
+    double2* __restrict__ slots_a, double2* __restrict__ slots_b, double4* sP,
+    double2 (*sX)[3 * NV], double2 (*sAcc)[32][3 * NV], double2 (*sRed)[3 * NV]) {
+  if (I == J)
+    sym64_superblock_pair_t<NV, true>(n, pos, xa_v, xb_v, k, inv_k, s0, I, J, slots_a, slots_b,
+                                      sP, sX, sAcc, sRed);
+  else
+    sym64_superblock_pair_t<NV, false>(n, pos, xa_v, xb_v, k, inv_k, s0, I, J, slots_a, slots_b,
+                                       sP, sX, sAcc, sRed);
 }
 
 __global__ void __launch_bounds__(kSym64Threads, 1)
