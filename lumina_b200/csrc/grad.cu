@@ -272,13 +272,16 @@ int lum_grad_cext(lum_session* s, const double direction[3], const double polari
   cudaStream_t st = s->stream;
   const int n = op.n;
   const size_t len = 3 * (size_t)n;
-  DevBuf E, Ec, P, Mu, part, dinv, gr, ge;
-  LUM_TRY(E.alloc(sizeof(double2) * len));
-  LUM_TRY(Ec.alloc(sizeof(double2) * len));
-  LUM_TRY(P.alloc(sizeof(double2) * len));
-  LUM_TRY(Mu.alloc(sizeof(double2) * len));
-  LUM_TRY(gr.alloc(sizeof(double) * len));
-  if (grad_eps) LUM_TRY(ge.alloc(sizeof(double) * 2 * (size_t)n));
+  // workspaces kept by the session: no allocation once they have grown
+  auto grow = [](DevBuf& b, size_t bytes) { return b.bytes >= bytes ? LUM_OK : b.alloc(bytes); };
+  DevBuf &E = s->gE, &Ec = s->gEc, &P = s->gP, &Mu = s->gMu, &part = s->gPart,
+         &dinv = s->gDinv, &gr = s->gR, &ge = s->gEps;
+  LUM_TRY(grow(E, sizeof(double2) * len));
+  LUM_TRY(grow(Ec, sizeof(double2) * len));
+  LUM_TRY(grow(P, sizeof(double2) * len));
+  LUM_TRY(grow(Mu, sizeof(double2) * len));
+  LUM_TRY(grow(gr, sizeof(double) * len));
+  if (grad_eps) LUM_TRY(grow(ge, sizeof(double) * 2 * (size_t)n));
   if (dinv_alpha_deps) {
     std::vector<double> h(18 * (size_t)n);
     for (int i = 0; i < n; ++i)
@@ -286,8 +289,9 @@ int lum_grad_cext(lum_session* s, const double direction[3], const double polari
         h[2 * ((size_t)e * n + i)] = dinv_alpha_deps[18 * (size_t)i + 2 * e];
         h[2 * ((size_t)e * n + i) + 1] = dinv_alpha_deps[18 * (size_t)i + 2 * e + 1];
       }
-    LUM_TRY(dinv.alloc(sizeof(double) * h.size()));
-    LUM_TRY_CUDA(cudaMemcpyAsync(dinv.p, h.data(), dinv.bytes, cudaMemcpyHostToDevice, st));
+    LUM_TRY(grow(dinv, sizeof(double) * h.size()));
+    LUM_TRY_CUDA(cudaMemcpyAsync(dinv.p, h.data(), sizeof(double) * h.size(),
+                                 cudaMemcpyHostToDevice, st));
     LUM_TRY_CUDA(cudaStreamSynchronize(st));  // h is freed on scope exit
   }
   const double2 e0 = make_double2(amplitude * polarisation[0], amplitude * polarisation[1]);
@@ -312,7 +316,7 @@ int lum_grad_cext(lum_session* s, const double direction[3], const double polari
   int ns = std::max(1, std::min(32, (4 * sms + tiles - 1) / tiles));
   const int chunk = ((tiles + ns - 1) / ns) * kGradBlock;
   ns = (n + chunk - 1) / chunk;
-  LUM_TRY(part.alloc(sizeof(double2) * (size_t)ns * len));
+  LUM_TRY(grow(part, sizeof(double2) * (size_t)ns * len));
   grad_pairs<<<dim3(tiles, ns), kGradBlock, 0, st>>>(n, op.pos64.as<double4>(), P.as<double2>(),
                                                      Mu.as<double2>(), op.k, chunk,
                                                      part.as<double2>());
@@ -321,15 +325,18 @@ int lum_grad_cext(lum_session* s, const double direction[3], const double polari
   grad_finish<<<(n + 127) / 128, 128, 0, st>>>(
       n, op.pos64.as<double4>(), P.as<double2>(), Mu.as<double2>(), E.as<double2>(), op.k,
       direction[0], direction[1], direction[2], part.as<double2>(), ns,
-      op.use_fcd ? op.ell_w : 0, op.near_j.as<int>(), op.cell, dinv.as<double2>(), scale,
+      op.use_fcd ? op.ell_w : 0, op.near_j.as<int>(), op.cell,
+      dinv_alpha_deps ? dinv.as<double2>() : nullptr, scale,
       gr.as<double>(), grad_eps ? ge.as<double>() : nullptr);
   LUM_CHECK_LAUNCH();
   std::vector<double> hp(2 * len), he(2 * len);
-  LUM_TRY_CUDA(cudaMemcpyAsync(hp.data(), P.p, P.bytes, cudaMemcpyDeviceToHost, st));
-  LUM_TRY_CUDA(cudaMemcpyAsync(he.data(), E.p, E.bytes, cudaMemcpyDeviceToHost, st));
-  LUM_TRY_CUDA(cudaMemcpyAsync(grad_r, gr.p, gr.bytes, cudaMemcpyDeviceToHost, st));
+  // exact sizes: the session's workspaces may be larger than this system
+  LUM_TRY_CUDA(cudaMemcpyAsync(hp.data(), P.p, sizeof(double2) * len, cudaMemcpyDeviceToHost, st));
+  LUM_TRY_CUDA(cudaMemcpyAsync(he.data(), E.p, sizeof(double2) * len, cudaMemcpyDeviceToHost, st));
+  LUM_TRY_CUDA(cudaMemcpyAsync(grad_r, gr.p, sizeof(double) * len, cudaMemcpyDeviceToHost, st));
   if (grad_eps)
-    LUM_TRY_CUDA(cudaMemcpyAsync(grad_eps, ge.p, ge.bytes, cudaMemcpyDeviceToHost, st));
+    LUM_TRY_CUDA(cudaMemcpyAsync(grad_eps, ge.p, sizeof(double) * 2 * (size_t)n,
+                                 cudaMemcpyDeviceToHost, st));
   LUM_TRY_CUDA(cudaStreamSynchronize(st));
   // C_ext = k/|E0|^2 sum Im(conj(E) . p)  (cda/mod.rs:196-203)
   double acc = 0.0;

@@ -438,6 +438,10 @@ struct lum_session {
   lum_status apply2(int precision, const double2* x, const double2* x2, double2* y, double2* y2,
                     const int* skip, const int* skip2);
   lum::GmresWork gw2;           // workspace of the second right-hand side
+  // lum_grad_cext workspaces (incident field and its conjugate, forward and
+  // adjoint solutions, pair partials, d alpha^-1 / d eps, outputs); they
+  // grow on demand and live with the session
+  lum::DevBuf gE, gEc, gP, gMu, gPart, gDinv, gR, gEps;
 };
 
 // Device GMRES drivers (gmres.cu): one right-hand side, or one or two in

@@ -1028,14 +1028,14 @@ static void sym_launch_t(const OtfOperator& o, const double2* x, const int* skip
 #undef LUM_SYM_LAUNCH
 }
 
-template <int MINB, int RP>
+template <int MINB, int RP, int UNR = 1>
 static void sym2_launch_t(const OtfOperator& o, const double2* x, const double2* x2,
                           const int* skip, const int* skip2, cudaStream_t st) {
   const float kf = (float)o.k, s0f = (float)(o.k * o.k * o.k / (4.0 * kPi));
   float2* s1 = o.sym_slots.as<float2>();
   float2* s2 = s1 + (size_t)o.sym_nb * 3 * (size_t)o.n;
 #define LUM_SYM2_LAUNCH(F, L)                                                                 \
-  otf_pairs_f32_sym2<F, L, MINB, RP><<<o.sym_nitems, SymShape<RP>::kThreads, 0, st>>>(        \
+  otf_pairs_f32_sym2<F, L, MINB, RP, UNR><<<o.sym_nitems, SymShape<RP>::kThreads, 0, st>>>(   \
       o.n, o.pos_hi.as<float4>(), o.pos_lo.as<float4>(), x, x2, kf, s0f,                     \
       o.sym_items.as<int2>(), s1, s2, skip, skip2)
   if (o.fast_trig && o.lofree)
@@ -1051,8 +1051,8 @@ static void sym2_launch_t(const OtfOperator& o, const double2* x, const double2*
 
 namespace {
 // Builds of the symmetric FP32 scheme the tuner chooses from: rows per
-// thread (2 or 4) x CTAs per SM (the register cap).  f32_sym is 1 + the
-// index into this table, 0 for the split kernels.
+// thread (2, 4 or 8) x CTAs per SM (the register cap) x unroll of the step
+// loop.  f32_sym is 1 + the index into this table, 0 for the split kernels.
 struct SymVariantEntry {
   const char* name;
   void (*launch)(const OtfOperator&, const double2*, const int*, cudaStream_t);
@@ -1082,6 +1082,7 @@ const Sym2VariantEntry kSym2Variants[] = {
     {"sym2_rows2_minb2", sym2_launch_t<2, 1>},
     {"sym2_rows2_minb1", sym2_launch_t<1, 1>},
     {"sym2_rows4_minb2", sym2_launch_t<2, 2>},
+    {"sym2_rows4_minb2_unroll2", sym2_launch_t<2, 2, 2>},
 };
 constexpr int kNumSym2Variants = sizeof(kSym2Variants) / sizeof(kSym2Variants[0]);
 }  // namespace
@@ -1376,8 +1377,9 @@ lum_status OtfOperator::tune_f32_x2(cudaStream_t st) {
   // LUMINA_F32_SYM=v forces symmetric build v here too (the two-vector build
   // of that number, capped at the last), =0 excludes the symmetric scheme
   const char* sym_env = std::getenv("LUMINA_F32_SYM");
-  if (isolated && sym_env && sym_env[0] >= '1' && sym_env[0] <= '9') {
-    f32x2_sym = std::min(sym_env[0] - '0', kNumSym2Variants);
+  const int sym_forced = sym_env ? std::atoi(sym_env) : 0;
+  if (isolated && sym_forced >= 1) {
+    f32x2_sym = std::min(sym_forced, kNumSym2Variants);
     return sym_prepare(st);
   }
   const bool sym_allowed = isolated && !(sym_env && sym_env[0] == '0');
@@ -1597,7 +1599,7 @@ batch_pairs_f32(BatchGeom g, const double2* __restrict__ x, const int4* __restri
 // superblock pairs of each system (pairs_f32_sym.cuh), written to per-system
 // slots laid out like the split partials, [superblock][3N] over the global
 // dipole range, so the batch epilogue sums sys_nb[s] of them per row.
-template <bool FAST, bool LOFREE, int MINB, int RP>
+template <bool FAST, bool LOFREE, int MINB, int RP, int UNR = 1>
 __global__ void __launch_bounds__(SymShape<RP>::kThreads, MINB)
 batch_pairs_f32_sym(BatchGeom g, const double2* __restrict__ x, const int4* __restrict__ items,
                     int nitems, unsigned* counters, const BatchFlags* __restrict__ flags,
@@ -1613,7 +1615,7 @@ batch_pairs_f32_sym(BatchGeom g, const double2* __restrict__ x, const int4* __re
     if (batch_skipped(flags, s, skip_mode)) continue;  // CTA-uniform
     const int off = g.sys_off[s], n = g.sys_off[s + 1] - off;
     const double k = g.sys_k[s];
-    sym_superblock_pair<FAST, LOFREE, RP, 1>(
+    sym_superblock_pair<FAST, LOFREE, RP, 1, UNR>(
         n, g.hi + off, g.lo + off, x + 3 * (size_t)off, nullptr, (float)k,
         (float)(k * k * k / (4.0 * kPi)), item.y, item.z, slots + 3 * (size_t)off, nullptr,
         stride, sS, sAcc, sRed);
@@ -1796,13 +1798,14 @@ lum_status batch_near_fcd(BatchGeom& g, int use_fcd, DevBuf& near_j, DevBuf& fcd
 }
 
 // Builds of the batched symmetric kernel (g.sym32 = 1 + index): 2 rows per
-// thread at 2 CTAs per SM, or 4 rows per thread at 4 CTAs per SM.
-template <int MINB, int RP>
+// thread at 2 CTAs per SM, 4 rows per thread at 4 CTAs per SM, and 4 rows
+// with the step loop unrolled (4 CTAs by two, 3 CTAs by four).
+template <int MINB, int RP, int UNR = 1>
 static void batch_sym_launch_t(const BatchGeom& g, const double2* x, const BatchQueue& q,
                                const BatchFlags* flags, int skip_mode, float2* slots,
                                cudaStream_t st) {
 #define LUM_BSYM(F, L)                                                                       \
-  batch_pairs_f32_sym<F, L, MINB, RP><<<q.grid, SymShape<RP>::kThreads, 0, st>>>(            \
+  batch_pairs_f32_sym<F, L, MINB, RP, UNR><<<q.grid, SymShape<RP>::kThreads, 0, st>>>(       \
       g, x, q.items.as<int4>(), q.nitems, q.counters.as<unsigned>(), flags, skip_mode, slots)
   if (g.fast && g.lofree)
     LUM_BSYM(true, true);
@@ -1815,21 +1818,21 @@ static void batch_sym_launch_t(const BatchGeom& g, const double2* x, const Batch
 #undef LUM_BSYM
 }
 
-template <int MINB, int RP>
+template <int MINB, int RP, int UNR = 1>
 static int batch_sym_occupancy_t(const BatchGeom& g) {
   int occ = 1;
   if (g.fast && g.lofree)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_pairs_f32_sym<true, true, MINB, RP>,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_pairs_f32_sym<true, true, MINB, RP, UNR>,
                                                   SymShape<RP>::kThreads, 0);
   else if (g.fast)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_pairs_f32_sym<true, false, MINB, RP>,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_pairs_f32_sym<true, false, MINB, RP, UNR>,
                                                   SymShape<RP>::kThreads, 0);
   else if (g.lofree)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_pairs_f32_sym<false, true, MINB, RP>,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_pairs_f32_sym<false, true, MINB, RP, UNR>,
                                                   SymShape<RP>::kThreads, 0);
   else
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &occ, batch_pairs_f32_sym<false, false, MINB, RP>, SymShape<RP>::kThreads, 0);
+        &occ, batch_pairs_f32_sym<false, false, MINB, RP, UNR>, SymShape<RP>::kThreads, 0);
   return std::max(1, occ);
 }
 
@@ -1843,6 +1846,10 @@ struct BatchSymVariant {
 const BatchSymVariant kBatchSym[] = {
     {"batch_sym_rows2_minb2", batch_sym_launch_t<2, 1>, batch_sym_occupancy_t<2, 1>},
     {"batch_sym_rows4_minb4", batch_sym_launch_t<4, 2>, batch_sym_occupancy_t<4, 2>},
+    {"batch_sym_rows4_minb4_unroll2", batch_sym_launch_t<4, 2, 2>,
+     batch_sym_occupancy_t<4, 2, 2>},
+    {"batch_sym_rows4_minb3_unroll4", batch_sym_launch_t<3, 2, 4>,
+     batch_sym_occupancy_t<3, 2, 4>},
 };
 constexpr int kNumBatchSym = sizeof(kBatchSym) / sizeof(kBatchSym[0]);
 }  // namespace

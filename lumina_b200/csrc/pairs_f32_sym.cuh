@@ -359,7 +359,7 @@ otf_pairs_f32_sym(int n, const float4* __restrict__ obs_hi, const float4* __rest
 
 // Two vectors (see NV above).  A vector whose skip flag is set is left out;
 // with both set the kernel returns at once.
-template <bool FAST, bool LOFREE, int MINB, int RP>
+template <bool FAST, bool LOFREE, int MINB, int RP, int UNR = 1>
 __global__ void __launch_bounds__(SymShape<RP>::kThreads, MINB)
 otf_pairs_f32_sym2(int n, const float4* __restrict__ obs_hi, const float4* __restrict__ obs_lo,
                    const double2* __restrict__ x, const double2* __restrict__ x2, float k,
@@ -373,12 +373,12 @@ otf_pairs_f32_sym2(int n, const float4* __restrict__ obs_hi, const float4* __res
   __shared__ float sRed[32 * 12];
   const int2 it = items[blockIdx.x];
   if (live && live2)
-    sym_superblock_pair<FAST, LOFREE, RP, 2>(n, obs_hi, obs_lo, x, x2, k, s0, it.x, it.y, slots,
-                                             slots2, 3 * (size_t)n, sS, sAcc, sRed);
+    sym_superblock_pair<FAST, LOFREE, RP, 2, UNR>(n, obs_hi, obs_lo, x, x2, k, s0, it.x, it.y,
+                                                  slots, slots2, 3 * (size_t)n, sS, sAcc, sRed);
   else
-    sym_superblock_pair<FAST, LOFREE, RP, 1>(n, obs_hi, obs_lo, live ? x : x2, nullptr, k, s0,
-                                             it.x, it.y, live ? slots : slots2, nullptr,
-                                             3 * (size_t)n, sS, sAcc, sRed);
+    sym_superblock_pair<FAST, LOFREE, RP, 1, UNR>(n, obs_hi, obs_lo, live ? x : x2, nullptr, k,
+                                                  s0, it.x, it.y, live ? slots : slots2, nullptr,
+                                                  3 * (size_t)n, sS, sAcc, sRed);
 }
 
 }  // namespace lum

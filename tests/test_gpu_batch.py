@@ -167,7 +167,7 @@ def test_batch_rejects_invalid_input(backend):
         backend.create_batch([(bad, inv, 0.01, 1.5)])
 
 
-@pytest.mark.parametrize("variant", ["1", "2"])
+@pytest.mark.parametrize("variant", ["1", "2", "3", "4"])
 def test_batch_symmetric_scheme_matches_oracle(backend, rng, monkeypatch, variant):
     """The symmetric FP32 scheme over the batch (each unordered pair once per
     system, superblock pairs drawn from one work list; LUMINA_BATCH_SYM=v

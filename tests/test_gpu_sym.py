@@ -22,7 +22,7 @@ from tests.conftest import rand_vec, rel_err
 pytestmark = pytest.mark.gpu
 
 SYM_VARIANTS = ("1", "2", "3", "4", "5", "6", "7", "8", "9", "10", "11")
-SYM2_VARIANTS = ("1", "2", "3")
+SYM2_VARIANTS = ("1", "2", "3", "4")
 
 
 def _cases(rng):
