@@ -660,14 +660,18 @@ int lum_session_matvec_device(lum_session* s, int precision, const void* x, void
   return st;
 }
 
+// Host-path staging buffers of a session: grown on demand and kept, since a
+// cudaMalloc / cudaFree pair per call costs far more than the copies.
+static lum_status grow_buf(lum::DevBuf& b, size_t bytes) {
+  return b.bytes >= bytes ? LUM_OK : b.alloc(bytes);
+}
+
 int lum_session_matvec(lum_session* s, int precision, const double* x, double* y) {
   if (bad_ptr(s, "session") || bad_ptr(x, "x") || bad_ptr(y, "y")) return LUM_ERR_INVALID;
   cudaSetDevice(s->ctx->device);
   const size_t bytes = sizeof(double2) * (size_t)s->dim;
-  if (!s->xbuf.p) {
-    LUM_TRY(s->xbuf.alloc(bytes));
-    LUM_TRY(s->ybuf.alloc(bytes));
-  }
+  LUM_TRY(grow_buf(s->xbuf, bytes));
+  LUM_TRY(grow_buf(s->ybuf, bytes));
   LUM_TRY_CUDA(cudaMemcpyAsync(s->xbuf.p, x, bytes, cudaMemcpyHostToDevice, s->stream));
   LUM_TRY(s->apply(precision, s->xbuf.as<double2>(), s->ybuf.as<double2>()));
   LUM_TRY_CUDA(cudaMemcpyAsync(y, s->ybuf.p, bytes, cudaMemcpyDeviceToHost, s->stream));
@@ -715,13 +719,12 @@ int lum_session_matmul_vectors(lum_session* s, const double* X, double* Y, int n
   LUM_TRY(check_matmul(s, X, Y, nrhs, method));
   cudaSetDevice(s->ctx->device);
   const size_t bytes = sizeof(double2) * (size_t)s->dim * nrhs;
-  lum::DevBuf dx, dy;
-  LUM_TRY(dx.alloc(bytes));
-  LUM_TRY(dy.alloc(bytes));
-  LUM_TRY_CUDA(cudaMemcpyAsync(dx.p, X, bytes, cudaMemcpyHostToDevice, s->stream));
-  LUM_TRY(s->cached.apply_multi(dx.as<double2>(), dy.as<double2>(), nrhs, 1, s->dim, method,
-                                s->stream));
-  LUM_TRY_CUDA(cudaMemcpyAsync(Y, dy.p, bytes, cudaMemcpyDeviceToHost, s->stream));
+  LUM_TRY(grow_buf(s->xbuf, bytes));
+  LUM_TRY(grow_buf(s->ybuf, bytes));
+  LUM_TRY_CUDA(cudaMemcpyAsync(s->xbuf.p, X, bytes, cudaMemcpyHostToDevice, s->stream));
+  LUM_TRY(s->cached.apply_multi(s->xbuf.as<double2>(), s->ybuf.as<double2>(), nrhs, 1, s->dim,
+                                method, s->stream));
+  LUM_TRY_CUDA(cudaMemcpyAsync(Y, s->ybuf.p, bytes, cudaMemcpyDeviceToHost, s->stream));
   LUM_TRY_CUDA(cudaStreamSynchronize(s->stream));
   return lum::cgemm_status(s->cached, s->stream);
 }
@@ -768,14 +771,13 @@ int lum_solve_gmres_multi(lum_session* s, int nrhs, const double* b, double tol,
   }
   cudaSetDevice(s->ctx->device);
   const size_t bytes = sizeof(double2) * (size_t)s->dim * nrhs;
-  DevBuf bd, xd;
-  LUM_TRY(bd.alloc(bytes));
-  LUM_TRY(xd.alloc(bytes));
-  LUM_TRY_CUDA(cudaMemcpyAsync(bd.p, b, bytes, cudaMemcpyHostToDevice, s->stream));
-  int st = lum_solve_gmres_multi_device(s, nrhs, bd.p, xd.p, tol, max_iter, restart, mode, info,
-                                        nullptr);
+  LUM_TRY(grow_buf(s->bbuf, bytes));
+  LUM_TRY(grow_buf(s->xbuf, bytes));
+  LUM_TRY_CUDA(cudaMemcpyAsync(s->bbuf.p, b, bytes, cudaMemcpyHostToDevice, s->stream));
+  int st = lum_solve_gmres_multi_device(s, nrhs, s->bbuf.p, s->xbuf.p, tol, max_iter, restart,
+                                        mode, info, nullptr);
   if (st == LUM_OK || st == LUM_ERR_NOT_CONVERGED) {
-    LUM_TRY_CUDA(cudaMemcpyAsync(x, xd.p, bytes, cudaMemcpyDeviceToHost, s->stream));
+    LUM_TRY_CUDA(cudaMemcpyAsync(x, s->xbuf.p, bytes, cudaMemcpyDeviceToHost, s->stream));
     LUM_TRY_CUDA(cudaStreamSynchronize(s->stream));
   }
   return st;
@@ -804,11 +806,9 @@ int lum_solve_gmres(lum_session* s, const double* b, double tol, int max_iter, i
   if (bad_ptr(s, "session") || bad_ptr(b, "b") || bad_ptr(x, "x")) return LUM_ERR_INVALID;
   cudaSetDevice(s->ctx->device);
   const size_t bytes = sizeof(double2) * (size_t)s->dim;
-  if (!s->bbuf.p) LUM_TRY(s->bbuf.alloc(bytes));
-  if (!s->xbuf.p) {
-    LUM_TRY(s->xbuf.alloc(bytes));
-    LUM_TRY(s->ybuf.alloc(bytes));
-  }
+  LUM_TRY(grow_buf(s->bbuf, bytes));
+  LUM_TRY(grow_buf(s->xbuf, bytes));
+  LUM_TRY(grow_buf(s->ybuf, bytes));
   LUM_TRY_CUDA(cudaMemcpyAsync(s->bbuf.p, b, bytes, cudaMemcpyHostToDevice, s->stream));
   int st = lum_solve_gmres_device(s, s->bbuf.p, s->xbuf.p, tol, max_iter, restart, mode, info,
                                   nullptr);
