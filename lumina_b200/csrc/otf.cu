@@ -823,6 +823,7 @@ lum_status OtfOperator::set_physics(double k_, const double* inv_alpha_host, int
   }
   k = k_;
   if (first) {
+    LUM_TRY(sincos_table_ready());  // the FP64 symmetric kernels' sin / cos table
     use_fcd = use_fcd_;
     cell = cell_;
     has_lattice = lat != nullptr;

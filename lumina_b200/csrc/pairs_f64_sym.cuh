@@ -2,7 +2,8 @@
 // pair once (the FP64 counterpart of pairs_f32_sym.cuh).
 //
 // G(r_i - r_j) = G(r_j - r_i) = G^T (greens.rs:34-71), so the pair scalars
-// (A, B', d) -- one rsqrt and one sincos, software sequences in FP64 -- serve
+// (A, B', d) -- one rsqrt and one sincos in FP64 (the table-driven sincos of
+// device_sincos.cuh) -- serve
 // both y_i += G x_j and y_j += G x_i.  The FP64 pipe is the bound; halving
 // the transcendental sequences per ordered pair is the point.
 //
@@ -23,6 +24,8 @@
 // before the single store of slot I.
 #pragma once
 
+#include "device_sincos.cuh"
+
 namespace lum {
 
 constexpr int kSym64Threads = kSymRows;  // one row per thread
@@ -32,7 +35,8 @@ __device__ __forceinline__ void sym64_superblock_pair_t(
     int n, const double4* __restrict__ pos, const double2* __restrict__ xa_v,
     const double2* __restrict__ xb_v, double k, double inv_k, double s0, int I, int J,
     double2* __restrict__ slots_a, double2* __restrict__ slots_b, double4* sP,
-    double2 (*sX)[3 * NV], double2 (*sAcc)[32][3 * NV], double2 (*sRed)[3 * NV]) {
+    double2 (*sX)[3 * NV], double2 (*sAcc)[32][3 * NV], double2 (*sRed)[3 * NV],
+    const double2* sTab) {
   constexpr int kWarps = kSym64Threads / 32;
   constexpr int kHalf = kWarps / 2;
   const double2* xv[2] = {xa_v, xb_v};
@@ -89,7 +93,7 @@ __device__ __forceinline__ void sym64_superblock_pair_t(
       const double u = ir * inv_k;
       const double u2 = u * u;
       double sn, cs;
-      sincos(k * Rr, &sn, &cs);
+      sincos_tab(k * Rr, sTab, &sn, &cs);
       const double su = drop ? 0.0 : s0 * u;
       const double pr = su * cs, pi = su * sn;
       const double ar = 1.0 - u2;
@@ -195,13 +199,14 @@ __device__ __forceinline__ void sym64_superblock_pair(
     int n, const double4* __restrict__ pos, const double2* __restrict__ xa_v,
     const double2* __restrict__ xb_v, double k, double inv_k, double s0, int I, int J,
     double2* __restrict__ slots_a, double2* __restrict__ slots_b, double4* sP,
-    double2 (*sX)[3 * NV], double2 (*sAcc)[32][3 * NV], double2 (*sRed)[3 * NV]) {
+    double2 (*sX)[3 * NV], double2 (*sAcc)[32][3 * NV], double2 (*sRed)[3 * NV],
+    const double2* sTab) {
   if (I == J)
     sym64_superblock_pair_t<NV, true>(n, pos, xa_v, xb_v, k, inv_k, s0, I, J, slots_a, slots_b,
-                                      sP, sX, sAcc, sRed);
+                                      sP, sX, sAcc, sRed, sTab);
   else
     sym64_superblock_pair_t<NV, false>(n, pos, xa_v, xb_v, k, inv_k, s0, I, J, slots_a, slots_b,
-                                       sP, sX, sAcc, sRed);
+                                       sP, sX, sAcc, sRed, sTab);
 }
 
 __global__ void __launch_bounds__(kSym64Threads, 1)
@@ -213,9 +218,11 @@ otf_pairs_f64_sym(int n, const double4* __restrict__ pos, const double2* __restr
   __shared__ double2 sX[32][3];
   __shared__ double2 sAcc[kSym64Threads / 64][32][3];
   __shared__ double2 sRed[32][3];
+  __shared__ double2 sTab[kScTab];
+  sincos_table_stage(sTab);  // the first group's barrier precedes its use
   const int2 it = items[blockIdx.x];
   sym64_superblock_pair<1>(n, pos, x, nullptr, k, inv_k, s0, it.x, it.y, slots, nullptr, sP, sX,
-                           sAcc, sRed);
+                           sAcc, sRed, sTab);
 }
 
 // Two vectors; a vector whose skip flag is set is left out, with both set
@@ -232,17 +239,19 @@ otf_pairs_f64_sym2(int n, const double4* __restrict__ pos, const double2* __rest
   __shared__ double2 sX[32][6];
   __shared__ double2 sAcc[kSym64Threads / 64][32][6];
   __shared__ double2 sRed[32][6];
+  __shared__ double2 sTab[kScTab];
+  sincos_table_stage(sTab);  // the first group's barrier precedes its use
   const int2 it = items[blockIdx.x];
   if (live && live2) {
     sym64_superblock_pair<2>(n, pos, x, x2, k, inv_k, s0, it.x, it.y, slots, slots2, sP, sX,
-                             sAcc, sRed);
+                             sAcc, sRed, sTab);
   } else {
     // the single-vector layout inside the same shared arrays
     sym64_superblock_pair<1>(n, pos, live ? x : x2, nullptr, k, inv_k, s0, it.x, it.y,
                              live ? slots : slots2, nullptr, sP,
                              reinterpret_cast<double2(*)[3]>(sX),
                              reinterpret_cast<double2(*)[32][3]>(sAcc),
-                             reinterpret_cast<double2(*)[3]>(sRed));
+                             reinterpret_cast<double2(*)[3]>(sRed), sTab);
   }
 }
 
