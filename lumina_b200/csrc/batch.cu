@@ -839,6 +839,7 @@ int lum_batch_create(lum_ctx* ctx, int n_systems, const int* sys_dipoles, const 
   cudaError_t ce = cudaSetDevice(ctx->device);
   if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking);
   if (ce != cudaSuccess) return fail(cuda_status(ce, "batch stream", __FILE__, __LINE__));
+  if (lum_status ts = otf_sincos_ready(); ts != LUM_OK) return fail(ts);
   cudaStream_t st = B->stream;
 
   // host-side layouts

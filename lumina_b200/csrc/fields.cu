@@ -18,6 +18,7 @@
 // plane grid on the host exactly as the reference does and evaluates it with
 // the near-field kernel.
 #include "lumina_internal.cuh"
+#include "device_sincos.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -37,6 +38,8 @@ near_field_part(int n, const double4* __restrict__ pos, const double2* __restric
                 double k, int m, const double4* __restrict__ obs, int chunk,
                 double2* __restrict__ part) {
   __shared__ SrcTile t;
+  __shared__ double2 sTab[kScTab];
+  sincos_table_stage(sTab);  // the first tile's barrier precedes its use
   const int q = blockIdx.x * kFieldBlock + threadIdx.x;
   const double4 o = obs[min(q, m - 1)];
   const int j0 = blockIdx.y * chunk, j1 = min(n, j0 + chunk);
@@ -60,7 +63,7 @@ near_field_part(int n, const double4* __restrict__ pos, const double2* __restric
       const double R = r2 * ir;
       const double u = ir * ik, u2 = u * u;
       double sn, cs;
-      sincos(k * R, &sn, &cs);
+      sincos_tab(k * R, sTab, &sn, &cs);
       const double qf = s0 * u;  // k^2 / (4 pi R)
       const double pr = qf * cs, pi = qf * sn;
       const double ar = 1.0 - u2;
@@ -116,6 +119,8 @@ __global__ void __launch_bounds__(kFieldBlock)
 far_field_part(int n, const double4* __restrict__ pos, const double2* __restrict__ mom,
                double k, int n_theta, int n_phi, int chunk, double2* __restrict__ part) {
   __shared__ SrcTile t;
+  __shared__ double2 sTab[kScTab];
+  sincos_table_stage(sTab);  // the first tile's barrier precedes its use
   const int m = n_theta * n_phi;
   const int q = min(blockIdx.x * kFieldBlock + (int)threadIdx.x, m - 1);
   const int it = q / n_phi, ip = q % n_phi;
@@ -139,7 +144,8 @@ far_field_part(int n, const double4* __restrict__ pos, const double2* __restrict
     for (int jj = 0; jj < cnt; ++jj) {
       const double4 r = t.pos[jj];
       double sn, cs;
-      sincos(rx * r.x + ry * r.y + rz * r.z, &sn, &cs);  // phase e^{-i k r.r_i} = cs - i sn
+      // phase e^{-i k r.r_i} = cs - i sn
+      sincos_tab(rx * r.x + ry * r.y + rz * r.z, sTab, &sn, &cs);
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         const double2 p = t.mom[c][jj];
@@ -226,6 +232,7 @@ lum_status near_field_device(lum_ctx* ctx, int n, const double* pos, const doubl
                              double k, const double dir[3], const double pol[3],
                              double amplitude, int m, const double* obs, double* field,
                              double* intensity) {
+  LUM_TRY(sincos_table_ready());
   cudaStream_t st = nullptr;
   LUM_TRY_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
   struct StreamGuard {
@@ -391,6 +398,7 @@ int lum_far_field(lum_ctx* ctx, int n, const double* pos, const double* moments,
     return LUM_ERR_INVALID;
   }
   LUM_TRY_CUDA(cudaSetDevice(ctx->device));
+  LUM_TRY(sincos_table_ready());
   cudaStream_t st = nullptr;
   LUM_TRY_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
   struct StreamGuard {

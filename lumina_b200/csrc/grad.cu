@@ -30,6 +30,7 @@
 // (C_ext is the imaginary part of a holomorphic function of eps).
 #include "lumina_internal.cuh"
 #include "device_physics.cuh"
+#include "device_sincos.cuh"
 
 #include <cmath>
 #include <vector>
@@ -60,11 +61,11 @@ struct Radial {
   double2 A, dA, B, dB;
 };
 
-__device__ __forceinline__ Radial radial(double R, double k) {
+__device__ __forceinline__ Radial radial(double R, double k, const double2* __restrict__ sTab) {
   const double ir = 1.0 / R, ir2 = ir * ir, ir3 = ir2 * ir, ir4 = ir2 * ir2, ir5 = ir4 * ir,
                ir6 = ir3 * ir3, k2 = k * k;
   double sn, cs;
-  sincos(k * R, &sn, &cs);
+  sincos_tab(k * R, sTab, &sn, &cs);
   const double f = 1.0 / (4.0 * kPi);
   const double2 e = make_double2(cs * f, sn * f);
   const double2 a = make_double2(k2 * ir - ir3, k * ir2);
@@ -82,9 +83,10 @@ __device__ __forceinline__ Radial radial(double R, double k) {
 // g_c += mu_i^T dG_c(d) p_j + mu_j^T dG_c(d) p_i, scaled by w.
 __device__ __forceinline__ void pair_grad(const double d[3], double k, const double2* mi,
                                           const double2* pi, const double2* mj,
-                                          const double2* pj, double w, double2 g[3]) {
+                                          const double2* pj, double w, double2 g[3],
+                                          const double2* __restrict__ sTab) {
   const double R = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
-  const Radial rf = radial(R, k);
+  const Radial rf = radial(R, k, sTab);
   const double2 mid = r_dot3(d, mi), pid = r_dot3(d, pi);
   const double2 mjd = r_dot3(d, mj), pjd = r_dot3(d, pj);
   const double2 s1 = c_add(c_dot3(mi, pj), c_dot3(mj, pi));
@@ -108,6 +110,8 @@ grad_pairs(int n, const double4* __restrict__ pos, const double2* __restrict__ p
            const double2* __restrict__ mu, double k, int chunk, double2* __restrict__ partial) {
   __shared__ double4 sP[kGradBlock];
   __shared__ double2 sPm[3 * kGradBlock], sMu[3 * kGradBlock];
+  __shared__ double2 sTab[kScTab];
+  sincos_table_stage(sTab);  // the first tile's barrier precedes its use
   const int tid = threadIdx.x;
   const int i = blockIdx.x * kGradBlock + tid;
   const int ic = min(i, n - 1);
@@ -132,7 +136,7 @@ grad_pairs(int n, const double4* __restrict__ pos, const double2* __restrict__ p
       if (jt + jj == i) continue;
       const double4 rj = sP[jj];
       const double d[3] = {ri.x - rj.x, ri.y - rj.y, ri.z - rj.z};
-      pair_grad(d, k, mi, pi, sMu + 3 * jj, sPm + 3 * jj, 1.0, g);
+      pair_grad(d, k, mi, pi, sMu + 3 * jj, sPm + 3 * jj, 1.0, g, sTab);
     }
   }
   if (i < n) {
@@ -150,6 +154,9 @@ grad_finish(int n, const double4* __restrict__ pos, const double2* __restrict__ 
             int ell_w, const int* __restrict__ near_j, double cell,
             const double2* __restrict__ dinv, double scale, double* __restrict__ grad_r,
             double* __restrict__ grad_eps) {
+  __shared__ double2 sTab[kScTab];
+  sincos_table_stage(sTab);
+  __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double2 pi[3] = {p[3 * i], p[3 * i + 1], p[3 * i + 2]};
@@ -180,13 +187,13 @@ grad_finish(int n, const double4* __restrict__ pos, const double2* __restrict__ 
           const double d[3] = {ro.x - px, ro.y - py, ro.z - pz};
           if (d[0] * d[0] + d[1] * d[1] + d[2] * d[2] < 1e-20) continue;
           const double wt = wts[ix] * wts[iy] * wts[iz];
-          pair_grad(d, k, mi, pi, mj, pj, wt, ga);
+          pair_grad(d, k, mi, pi, mj, pj, wt, ga, sTab);
           tw += wt;
         }
     const double inv = (tw > 1e-30) ? 1.0 / tw : 0.0;
     const double d0[3] = {ro.x - rs.x, ro.y - rs.y, ro.z - rs.z};
     for (int c = 0; c < 3; ++c) g[c] = c_add(g[c], c_scale(ga[c], inv));
-    pair_grad(d0, k, mi, pi, mj, pj, -1.0, g);
+    pair_grad(d0, k, mi, pi, mj, pj, -1.0, g, sTab);
   }
   // plane wave: i k dhat_c (mu_i . E_i - conj(E_i) . p_i)
   const double2 Ei[3] = {E[3 * i], E[3 * i + 1], E[3 * i + 2]};
@@ -269,6 +276,7 @@ int lum_grad_cext(lum_session* s, const double direction[3], const double polari
       return LUM_ERR_INVALID;
     }
   cudaSetDevice(s->ctx->device);
+  LUM_TRY(sincos_table_ready());
   cudaStream_t st = s->stream;
   const int n = op.n;
   const size_t len = 3 * (size_t)n;

@@ -380,6 +380,7 @@ int batch_occupancy(const BatchGeom& g, int precision);                         
 // Rows (and sources) of a superblock of the symmetric scheme; a system of n
 // dipoles has ceil(n / kBatchSymRows) superblocks and nb (nb + 1) / 2 items.
 constexpr int kBatchSymRows = 512;
+lum_status otf_sincos_ready();  // otf.cu: its FP64 pair kernels' sin / cos table
 lum_status batch_queue_sym(const std::vector<int>& off, int slots, BatchQueue& q,
                            std::vector<int>& nb, cudaStream_t st);                   // otf.cu
 int batch_sym_variants();                                                            // otf.cu

@@ -57,7 +57,8 @@ __device__ __forceinline__ void pairs_f64_cta(int n, const double4* __restrict__
                                               double2 m1, double2 m2, double z_mirror, double k,
                                               double inv_k, double s0, int row0, int j_begin,
                                               int j_end, double2* __restrict__ out,
-                                              double2* __restrict__ out2) {
+                                              double2* __restrict__ out2,
+                                              const double2* __restrict__ sTab) {
   __shared__ double4 sP[kOtfBlock];
   __shared__ double2 sX[3 * NR * kOtfBlock];
   const int tid = threadIdx.x;
@@ -107,7 +108,7 @@ __device__ __forceinline__ void pairs_f64_cta(int n, const double4* __restrict__
       double u = ir * inv_k;
       double u2 = u * u;
       double sn, cs;
-      sincos(k * Rr, &sn, &cs);
+      sincos_tab(k * Rr, sTab, &sn, &cs);
       double su = skip ? 0.0 : s0 * u;
       double pr = su * cs, pi = su * sn;
       double ar = 1.0 - u2;
@@ -158,10 +159,12 @@ otf_pairs_f64(int n, const double4* __restrict__ pos, const double2* __restrict_
               double s0, int chunk, double2* __restrict__ partial,
               const int* __restrict__ skip) {
   if (skip && *skip) return;
+  __shared__ double2 sTab[kScTab];
+  sincos_table_stage(sTab);  // the first source tile's barrier precedes its use
   const int j_begin = blockIdx.y * chunk;
   pairs_f64_cta<IMAGE, 1>(n, pos, x, nullptr, m0, m1, m2, z_mirror, k, inv_k, s0,
                           blockIdx.x * kOtfBlock, j_begin, min(n, j_begin + chunk),
-                          partial + (size_t)blockIdx.y * (3 * (size_t)n), nullptr);
+                          partial + (size_t)blockIdx.y * (3 * (size_t)n), nullptr, sTab);
 }
 
 // Two right-hand sides (see otf_pairs_f32_x2).
@@ -174,16 +177,18 @@ otf_pairs_f64_x2(int n, const double4* __restrict__ pos, const double2* __restri
                  const int* __restrict__ skip, const int* __restrict__ skip2) {
   const bool live = !(skip && *skip), live2 = !(skip2 && *skip2);
   if (!live && !live2) return;
+  __shared__ double2 sTab[kScTab];
+  sincos_table_stage(sTab);  // the first source tile's barrier precedes its use
   const int j_begin = blockIdx.y * chunk, j_end = min(n, j_begin + chunk);
   const size_t off = (size_t)blockIdx.y * (3 * (size_t)n);
   if (live && live2)
     pairs_f64_cta<IMAGE, 2>(n, pos, x, x2, m0, m1, m2, z_mirror, k, inv_k, s0,
                             blockIdx.x * kOtfBlock, j_begin, j_end, partial + off,
-                            partial2 + off);
+                            partial2 + off, sTab);
   else
     pairs_f64_cta<IMAGE, 1>(n, pos, live ? x : x2, nullptr, m0, m1, m2, z_mirror, k, inv_k, s0,
                             blockIdx.x * kOtfBlock, j_begin, j_end,
-                            (live ? partial : partial2) + off, nullptr);
+                            (live ? partial : partial2) + off, nullptr, sTab);
 }
 
 // ---------------------------------------------------------------------------
@@ -1628,6 +1633,8 @@ batch_pairs_f64(BatchGeom g, const double2* __restrict__ x, const int4* __restri
                 int nitems, unsigned* counters, const BatchFlags* __restrict__ flags,
                 int skip_mode, double2* __restrict__ partial) {
   __shared__ int s_item;
+  __shared__ double2 sTab[kScTab];
+  sincos_table_stage(sTab);  // staged once; the first tile's barrier precedes its use
   const size_t stride = 3 * (size_t)g.N;
   const double2 one = make_double2(1.0, 0.0);
   for (int it; (it = batch_draw(counters, nitems, &s_item)) >= 0;) {
@@ -1640,7 +1647,7 @@ batch_pairs_f64(BatchGeom g, const double2* __restrict__ x, const int4* __restri
     const double k = g.sys_k[s];
     pairs_f64_cta<false, 1>(n, g.pos64 + off, x + 3 * (size_t)off, nullptr, one, one, one, 0.0,
                             k, 1.0 / k, k * k * k / (4.0 * kPi), item.y, j0, j1,
-                            partial + (size_t)item.z * stride + 3 * (size_t)off, nullptr);
+                            partial + (size_t)item.z * stride + 3 * (size_t)off, nullptr, sTab);
   }
 }
 
@@ -1864,6 +1871,10 @@ int batch_sym_occupancy(const BatchGeom& g, int v) {
 }
 
 static_assert(kSymRows == kBatchSymRows, "one superblock size for the batch and its kernels");
+
+// The FP64 sin / cos table of this file's kernels, for callers outside it
+// (a cluster batch has no OtfOperator).
+lum_status otf_sincos_ready() { return sincos_table_ready(); }
 
 // Work list of the symmetric scheme: every superblock pair (I <= J) of every
 // system, ordered by decreasing cost (diagonal pairs count half).
