@@ -1075,6 +1075,8 @@ const SymVariantEntry kSymVariants[] = {
     {"sym_rows4_minb4_unroll2", sym_launch_t<4, 2, 2>},
     {"sym_rows4_minb3_unroll4", sym_launch_t<3, 2, 4>},
     {"sym_rows8_minb4_unroll2", sym_launch_t<4, 4, 2>},
+    {"sym_rows4_minb4_unroll4", sym_launch_t<4, 2, 4>},
+    {"sym_rows4_minb3_unroll8", sym_launch_t<3, 2, 8>},
 };
 constexpr int kNumSymVariants = sizeof(kSymVariants) / sizeof(kSymVariants[0]);
 

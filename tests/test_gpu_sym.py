@@ -3,7 +3,8 @@ once): every FP32 build of pairs_f32_sym.cuh, forced with LUMINA_F32_SYM=v
 (1: 2 rows per thread, 2 CTAs/SM; 2: 2 rows, 3 CTAs/SM; 3: 4 rows, 4 CTAs/SM;
 4: 4 rows, 3 CTAs/SM; 5, 6: builds 1 and 4 with the step loop unrolled by two;
 7, 8: 8 rows, 4 and 5 CTAs/SM; 9, 10, 11: 4 rows at 4 CTAs/SM unrolled by two,
-4 rows at 3 CTAs/SM unrolled by four, 8 rows at 4 CTAs/SM unrolled by two),
+4 rows at 3 CTAs/SM unrolled by four, 8 rows at 4 CTAs/SM unrolled by two; 12, 13:
+4 rows at 4 CTAs/SM unrolled by four, 4 rows at 3 CTAs/SM unrolled by eight),
 their two-vector builds, and the FP64 scheme of
 pairs_f64_sym.cuh, forced with LUMINA_F64_SYM=1, so that they run at sizes
 the oracle handles.  Tolerances: the FP32 bar 2e-5, the FP64 bar 1e-12."""
@@ -21,7 +22,7 @@ from tests.conftest import rand_vec, rel_err
 
 pytestmark = pytest.mark.gpu
 
-SYM_VARIANTS = ("1", "2", "3", "4", "5", "6", "7", "8", "9", "10", "11")
+SYM_VARIANTS = ("1", "2", "3", "4", "5", "6", "7", "8", "9", "10", "11", "12", "13")
 SYM2_VARIANTS = ("1", "2", "3", "4")
 
 
