@@ -21,6 +21,7 @@
 #include "device_sincos.cuh"
 
 #include <algorithm>
+#include <new>
 #include <cmath>
 
 namespace lum {
@@ -200,6 +201,23 @@ int field_splits(int blocks, int n, int sms) {
   return std::max(1, std::min(tiles, std::min(64, want)));
 }
 
+lum_status grow(DevBuf& b, size_t bytes) { return b.bytes >= bytes ? LUM_OK : b.alloc(bytes); }
+
+// The context's field workspace (created on first use; the caller has made
+// the context's device current).
+lum_status field_work(lum_ctx* ctx, FieldWork** out) {
+  static std::mutex create_mu;
+  std::lock_guard<std::mutex> lk(create_mu);
+  if (!ctx->fields) {
+    std::unique_ptr<FieldWork> fw(new (std::nothrow) FieldWork());
+    if (!fw) return LUM_ERR_OOM;
+    LUM_TRY_CUDA(cudaStreamCreateWithFlags(&fw->stream, cudaStreamNonBlocking));
+    ctx->fields = std::move(fw);
+  }
+  *out = ctx->fields.get();
+  return LUM_OK;
+}
+
 lum_status upload_sources(int n, const double* pos, const double* moments, DevBuf& dpos,
                           DevBuf& dmom, cudaStream_t st) {
   std::vector<double> p4(4 * (size_t)std::max(n, 1), 0.0);
@@ -217,8 +235,8 @@ lum_status upload_sources(int n, const double* pos, const double* moments, DevBu
       set_error("non-finite dipole moment at dipole %zu", q / 6);
       return LUM_ERR_INVALID;
     }
-  LUM_TRY(dpos.alloc(sizeof(double) * p4.size()));
-  LUM_TRY(dmom.alloc(sizeof(double2) * 3 * (size_t)std::max(n, 1)));
+  LUM_TRY(grow(dpos, sizeof(double) * p4.size()));
+  LUM_TRY(grow(dmom, sizeof(double2) * 3 * (size_t)std::max(n, 1)));
   LUM_TRY_CUDA(cudaMemcpyAsync(dpos.p, p4.data(), sizeof(double) * p4.size(),
                                cudaMemcpyHostToDevice, st));
   if (n > 0)
@@ -233,13 +251,12 @@ lum_status near_field_device(lum_ctx* ctx, int n, const double* pos, const doubl
                              double amplitude, int m, const double* obs, double* field,
                              double* intensity) {
   LUM_TRY(sincos_table_ready());
-  cudaStream_t st = nullptr;
-  LUM_TRY_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-  struct StreamGuard {
-    cudaStream_t s;
-    ~StreamGuard() { cudaStreamDestroy(s); }
-  } guard{st};
-  DevBuf dpos, dmom, dobs, dpart, dfield, dint;
+  FieldWork* fw = nullptr;
+  LUM_TRY(field_work(ctx, &fw));
+  std::lock_guard<std::mutex> lk(fw->mu);
+  cudaStream_t st = fw->stream;
+  DevBuf &dpos = fw->pos, &dmom = fw->mom, &dobs = fw->obs, &dpart = fw->part,
+         &dfield = fw->field, &dint = fw->inten;
   LUM_TRY(upload_sources(n, pos, moments, dpos, dmom, st));
   std::vector<double> o4(4 * (size_t)m, 0.0);
   for (int q = 0; q < m; ++q)
@@ -251,16 +268,16 @@ lum_status near_field_device(lum_ctx* ctx, int n, const double* pos, const doubl
       }
       o4[4 * (size_t)q + c] = v;
     }
-  LUM_TRY(dobs.alloc(sizeof(double) * o4.size()));
+  LUM_TRY(grow(dobs, sizeof(double) * o4.size()));
   LUM_TRY_CUDA(cudaMemcpyAsync(dobs.p, o4.data(), sizeof(double) * o4.size(),
                                cudaMemcpyHostToDevice, st));
   const int blocks = (m + kFieldBlock - 1) / kFieldBlock;
   const int ns = n > 0 ? field_splits(blocks, n, ctx->sms) : 0;
   const int chunk = ns > 0 ? ((n + ns - 1) / ns + kFieldBlock - 1) / kFieldBlock * kFieldBlock : 0;
   const int nsplit = ns > 0 ? (n + chunk - 1) / chunk : 0;
-  LUM_TRY(dpart.alloc(sizeof(double2) * 3 * (size_t)m * std::max(nsplit, 1)));
-  LUM_TRY(dfield.alloc(sizeof(double2) * 3 * (size_t)m));
-  if (intensity) LUM_TRY(dint.alloc(sizeof(double) * (size_t)m));
+  LUM_TRY(grow(dpart, sizeof(double2) * 3 * (size_t)m * std::max(nsplit, 1)));
+  LUM_TRY(grow(dfield, sizeof(double2) * 3 * (size_t)m));
+  if (intensity) LUM_TRY(grow(dint, sizeof(double) * (size_t)m));
   if (nsplit > 0) {
     near_field_part<<<dim3(blocks, nsplit), kFieldBlock, 0, st>>>(
         n, dpos.as<double4>(), dmom.as<double2>(), k, m, dobs.as<double4>(), chunk,
@@ -399,22 +416,21 @@ int lum_far_field(lum_ctx* ctx, int n, const double* pos, const double* moments,
   }
   LUM_TRY_CUDA(cudaSetDevice(ctx->device));
   LUM_TRY(sincos_table_ready());
-  cudaStream_t st = nullptr;
-  LUM_TRY_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-  struct StreamGuard {
-    cudaStream_t s;
-    ~StreamGuard() { cudaStreamDestroy(s); }
-  } guard{st};
-  DevBuf dpos, dmom, dpart, dth, dph, dint;
+  FieldWork* fw = nullptr;
+  LUM_TRY(field_work(ctx, &fw));
+  std::lock_guard<std::mutex> lk(fw->mu);
+  cudaStream_t st = fw->stream;
+  DevBuf &dpos = fw->pos, &dmom = fw->mom, &dpart = fw->part, &dth = fw->th, &dph = fw->ph,
+         &dint = fw->inten;
   LUM_TRY(upload_sources(n, pos, moments, dpos, dmom, st));
   const int blocks = (int)((m + kFieldBlock - 1) / kFieldBlock);
   const int ns = n > 0 ? field_splits(blocks, n, ctx->sms) : 0;
   const int chunk = ns > 0 ? ((n + ns - 1) / ns + kFieldBlock - 1) / kFieldBlock * kFieldBlock : 0;
   const int nsplit = ns > 0 ? (n + chunk - 1) / chunk : 0;
-  LUM_TRY(dpart.alloc(sizeof(double2) * 3 * m * std::max(nsplit, 1)));
-  LUM_TRY(dth.alloc(sizeof(double) * m));
-  LUM_TRY(dph.alloc(sizeof(double) * m));
-  LUM_TRY(dint.alloc(sizeof(double) * m));
+  LUM_TRY(grow(dpart, sizeof(double2) * 3 * m * std::max(nsplit, 1)));
+  LUM_TRY(grow(dth, sizeof(double) * m));
+  LUM_TRY(grow(dph, sizeof(double) * m));
+  LUM_TRY(grow(dint, sizeof(double) * m));
   if (nsplit > 0) {
     far_field_part<<<dim3(blocks, nsplit), kFieldBlock, 0, st>>>(
         n, dpos.as<double4>(), dmom.as<double2>(), k, n_theta, n_phi, chunk,

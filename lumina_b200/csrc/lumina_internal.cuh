@@ -19,6 +19,8 @@
 #include <string>
 #include <vector>
 #include <atomic>
+#include <memory>
+#include <mutex>
 
 #include "../../include/lumina_b200.h"
 
@@ -408,11 +410,25 @@ lum_status read_scalars(GmresWork& W, cudaStream_t st);
 }  // namespace lum
 
 // Session (opaque to callers).
+namespace lum {
+// Workspaces of a context's field entry points (fields.cu): one stream and
+// buffers that grow on demand, used by one caller at a time.
+struct FieldWork {
+  std::mutex mu;
+  cudaStream_t stream = nullptr;
+  DevBuf pos, mom, obs, part, field, inten, th, ph;
+  ~FieldWork() {
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+}  // namespace lum
+
 struct lum_ctx {
   int device = 0;
   std::string name;
   size_t mem_bytes = 0;
   int sms = 0;
+  std::unique_ptr<lum::FieldWork> fields;  // created by the first field call
 };
 
 struct lum_session {
