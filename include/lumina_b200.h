@@ -353,6 +353,10 @@ LUM_API int lum_solve_gmres_multi_device(lum_session* s, int nrhs, const void* b
                                          int mode, lum_solve_info* info, void* stream);
 
 /* ---- fields from solved moments (fields.rs) ------------------------------- */
+/* The field entry points and lum_harmonic_sources keep one stream and their
+ * device buffers with the context (grown on demand, freed by
+ * lum_ctx_destroy); calls on one context from several threads run one at a
+ * time. */
 /* field_at_point (crates/lumina-core/src/fields.rs:18-49) at m observation
  * points obs (3m doubles): E = E_inc + sum_i G(r - r_i) p_i, the point-dipole
  * tensor of greens.rs:34-71, dipoles with |r - r_i|^2 < 1e-20 skipped, FP64.

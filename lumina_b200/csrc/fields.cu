@@ -25,6 +25,20 @@
 #include <cmath>
 
 namespace lum {
+
+lum_status ctx_work(lum_ctx* ctx, FieldWork** out) {
+  static std::mutex create_mu;
+  std::lock_guard<std::mutex> lk(create_mu);
+  if (!ctx->fields) {
+    std::unique_ptr<FieldWork> fw(new (std::nothrow) FieldWork());
+    if (!fw) return LUM_ERR_OOM;
+    LUM_TRY_CUDA(cudaStreamCreateWithFlags(&fw->stream, cudaStreamNonBlocking));
+    ctx->fields = std::move(fw);
+  }
+  *out = ctx->fields.get();
+  return LUM_OK;
+}
+
 namespace {
 
 constexpr int kFieldBlock = 128;
@@ -203,20 +217,7 @@ int field_splits(int blocks, int n, int sms) {
 
 lum_status grow(DevBuf& b, size_t bytes) { return b.bytes >= bytes ? LUM_OK : b.alloc(bytes); }
 
-// The context's field workspace (created on first use; the caller has made
-// the context's device current).
-lum_status field_work(lum_ctx* ctx, FieldWork** out) {
-  static std::mutex create_mu;
-  std::lock_guard<std::mutex> lk(create_mu);
-  if (!ctx->fields) {
-    std::unique_ptr<FieldWork> fw(new (std::nothrow) FieldWork());
-    if (!fw) return LUM_ERR_OOM;
-    LUM_TRY_CUDA(cudaStreamCreateWithFlags(&fw->stream, cudaStreamNonBlocking));
-    ctx->fields = std::move(fw);
-  }
-  *out = ctx->fields.get();
-  return LUM_OK;
-}
+lum_status field_work(lum_ctx* ctx, FieldWork** out) { return ctx_work(ctx, out); }
 
 lum_status upload_sources(int n, const double* pos, const double* moments, DevBuf& dpos,
                           DevBuf& dmom, cudaStream_t st) {

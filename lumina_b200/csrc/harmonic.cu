@@ -67,17 +67,16 @@ int lum_harmonic_sources(lum_ctx* ctx, int order, int n, const double* local_fie
       return LUM_ERR_INVALID;
     }
   LUM_TRY_CUDA(cudaSetDevice(ctx->device));
-  cudaStream_t st = nullptr;
-  LUM_TRY_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-  struct StreamGuard {
-    cudaStream_t s;
-    ~StreamGuard() { cudaStreamDestroy(s); }
-  } guard{st};
-  DevBuf de, dc, dp;
+  FieldWork* fw = nullptr;
+  LUM_TRY(ctx_work(ctx, &fw));
+  std::lock_guard<std::mutex> lk(fw->mu);
+  cudaStream_t st = fw->stream;
+  DevBuf &de = fw->h_e, &dc = fw->h_chi, &dp = fw->h_p;
   const size_t vb = sizeof(double2) * 3 * (size_t)n, cb = sizeof(double2) * nc * (size_t)n_tensors;
-  LUM_TRY(de.alloc(vb));
-  LUM_TRY(dc.alloc(cb));
-  LUM_TRY(dp.alloc(vb));
+  auto grow = [](DevBuf& b, size_t bytes) { return b.bytes >= bytes ? LUM_OK : b.alloc(bytes); };
+  LUM_TRY(grow(de, vb));
+  LUM_TRY(grow(dc, cb));
+  LUM_TRY(grow(dp, vb));
   LUM_TRY_CUDA(cudaMemcpyAsync(de.p, local_fields, vb, cudaMemcpyHostToDevice, st));
   LUM_TRY_CUDA(cudaMemcpyAsync(dc.p, chi, cb, cudaMemcpyHostToDevice, st));
   const int per = n_tensors == n && n > 1 ? 1 : 0;

@@ -411,12 +411,14 @@ lum_status read_scalars(GmresWork& W, cudaStream_t st);
 
 // Session (opaque to callers).
 namespace lum {
-// Workspaces of a context's field entry points (fields.cu): one stream and
-// buffers that grow on demand, used by one caller at a time.
+// Workspaces of a context's own entry points (the fields of fields.cu, the
+// harmonic sources of harmonic.cu): one stream and buffers that grow on
+// demand, used by one caller at a time (hold mu).
 struct FieldWork {
   std::mutex mu;
   cudaStream_t stream = nullptr;
   DevBuf pos, mom, obs, part, field, inten, th, ph;
+  DevBuf h_e, h_chi, h_p;
   ~FieldWork() {
     if (stream) cudaStreamDestroy(stream);
   }
@@ -428,8 +430,14 @@ struct lum_ctx {
   std::string name;
   size_t mem_bytes = 0;
   int sms = 0;
-  std::unique_ptr<lum::FieldWork> fields;  // created by the first field call
+  std::unique_ptr<lum::FieldWork> fields;  // created by the first call that needs it
 };
+
+namespace lum {
+// The context's workspace, created on first use (fields.cu); the caller has
+// made the context's device current.
+lum_status ctx_work(lum_ctx* ctx, FieldWork** out);
+}  // namespace lum
 
 struct lum_session {
   lum_ctx* ctx = nullptr;
