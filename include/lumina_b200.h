@@ -48,6 +48,12 @@ typedef enum {
 
 /* Arithmetic of a matvec / matrix storage. */
 enum { LUM_FP64 = 0, LUM_FP32 = 1 };
+/* OR-ed into lum_session_assemble's storage precision: keep only the upper
+ * triangle of the matrix, as tiles of 192 x 192 entries (64 dipoles a side),
+ * for a free-space system, whose matrix is complex symmetric.  Half the
+ * device memory and half the bytes per product of dense rows.  No
+ * counterpart in the reference, which stores dense rows (gpu.rs:303-399). */
+enum { LUM_STORAGE_SYMMETRIC = 0x10 };
 
 /* Solve modes of lum_solve_gmres. */
 enum {
@@ -146,7 +152,13 @@ LUM_API int lum_session_upload_matrix(lum_session* s, const double* A);
 /* ComputeBackend::assemble_and_create_session (backend.rs:109-117,
  * gpu.rs:502-610), widened to the FCD / lattice / substrate terms of
  * assemble_interaction_matrix (assembly.rs:45-175): the whole 3N x 3N matrix
- * is built on the device.  inv_alpha = compute_diagonal_blocks output. */
+ * is built on the device.  inv_alpha = compute_diagonal_blocks output.
+ * storage_precision | LUM_STORAGE_SYMMETRIC stores the upper-triangle tiles
+ * only; INVALID with a lattice or a substrate (there A is not symmetric).
+ * Such a session applies its matrix one vector per product: a tensor-core
+ * product, or a lum_session_matmul_device of more than one vector, returns
+ * INVALID, and lum_session_matmul_vectors and the right-hand-side batches
+ * run one tile product per vector. */
 LUM_API int lum_session_assemble(lum_ctx* ctx, int n_dipoles, const double* pos,
                          const double* inv_alpha, double k, int use_fcd, double cell_size,
                          const lum_lattice* lattice, const double k_bloch[3],

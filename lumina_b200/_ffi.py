@@ -24,6 +24,7 @@ LUM_ERR_INVALID = 6
 
 LUM_FP64 = 0
 LUM_FP32 = 1
+LUM_STORAGE_SYMMETRIC = 0x10
 LUM_SOLVE_FP64 = 0
 LUM_SOLVE_FP32_REFINE = 1
 

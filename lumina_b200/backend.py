@@ -574,8 +574,14 @@ class CudaBackend:
 
     def assemble_and_create_session(self, positions, k: float, diagonal_blocks, use_fcd=False,
                                     cell_size=3.0, lattice=None, k_bloch=(0.0, 0.0, 0.0),
-                                    substrate=None, precision="fp32") -> CudaSession:
-        """Device-assembled dense session (backend.rs:109-117, widened)."""
+                                    substrate=None, precision="fp32",
+                                    symmetric=False) -> CudaSession:
+        """Device-assembled dense session (backend.rs:109-117, widened).
+
+        symmetric=True keeps only the upper-triangle tiles of the matrix
+        (LUM_STORAGE_SYMMETRIC): free-space systems only (no lattice, no
+        substrate), half the memory and half the bytes per product; products
+        run one vector at a time (no tensor-core path)."""
         pos = np.ascontiguousarray(np.asarray(positions, np.float64).reshape(-1, 3))
         n = pos.shape[0]
         ia = _c128(diagonal_blocks, 9 * n)
@@ -589,9 +595,10 @@ class CudaBackend:
                 _prec(precision), byref(h)), "assemble")
             return CudaSession(h, 3 * n, "cached", self)
         lat, sub = lattice_struct(lattice), substrate_struct(substrate)
+        storage = _prec(precision) | (_ffi.LUM_STORAGE_SYMMETRIC if symmetric else 0)
         _raise(self._lib.lum_session_assemble(self._h, n, _dp(pos), _dp(ia.view(np.float64)),
                                               float(k), int(bool(use_fcd)), float(cell_size),
-                                              _ref(lat), _dp(kb), _ref(sub), _prec(precision),
+                                              _ref(lat), _dp(kb), _ref(sub), storage,
                                               byref(h)), "assemble")
         return CudaSession(h, 3 * n, "cached", self)
 

@@ -664,8 +664,9 @@ lum_status batch_workspace(lum_batch* B, int m) {
 
 // y = A x for the K vectors of a right-hand-side batch.  An FP32-storage
 // cached matrix at FP32 takes the tensor-core product for all K vectors in
-// one launch; otherwise the session operator runs two vectors at a time
-// (the two-vector pair kernels for an on-the-fly session).
+// one launch; otherwise (symmetric tile storage included) the session
+// operator runs two vectors at a time (the two-vector pair kernels for an
+// on-the-fly session).
 lum_status rhs_apply(lum_batch* B, int prec, const double2* x, double2* y) {
   lum_session* s = B->src;
   const size_t n3 = (size_t)s->dim;
@@ -674,9 +675,9 @@ lum_status rhs_apply(lum_batch* B, int prec, const double2* x, double2* y) {
               "lum_session_set_sommerfeld after lum_session_set_wavelength");
     return LUM_ERR_INVALID;
   }
-  if (s->kind == 1 && s->cached.precision == LUM_FP32 && prec == LUM_FP32)
+  if (s->kind == 1 && !s->cached.packed && s->cached.precision == LUM_FP32 && prec == LUM_FP32)
     return s->cached.apply_multi(x, y, B->K, 1, (long long)n3, LUM_MATMUL_TENSOR, s->stream);
-  if (s->kind == 1 && s->cached.precision == LUM_FP64)
+  if (s->kind == 1 && !s->cached.packed && s->cached.precision == LUM_FP64)
     return s->cached.apply_multi(x, y, B->K, 1, (long long)n3, LUM_MATMUL_CUDA_CORES,
                                  s->stream);
   int r = 0;
@@ -1154,8 +1155,8 @@ int lum_batch_solve_device(lum_batch* B, const void* b_dev, void* x_dev, double 
   const long max_cycles = (long)std::max(max_iter, 0) + 1;
   // a tensor-core product whose pipeline wait gave up leaves tiles of its
   // result unwritten: the cycle's status is read after every cycle
-  const bool tensor = B->src && B->src->kind == 1 && B->src->cached.precision == LUM_FP32 &&
-                      mode == LUM_SOLVE_FP32_REFINE;
+  const bool tensor = B->src && B->src->kind == 1 && !B->src->cached.packed &&
+                      B->src->cached.precision == LUM_FP32 && mode == LUM_SOLVE_FP32_REFINE;
   // symmetric items of the systems still active (all of them at the start)
   long live = 0;
   if (!B->src)

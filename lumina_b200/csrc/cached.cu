@@ -98,6 +98,239 @@ __global__ void assemble_fcd(int n, int ell_w, const int* __restrict__ near_j,
     }
 }
 
+// ---------------------------------------------------------------------------
+// Symmetric tile storage.  Without a lattice sum or a substrate term the
+// matrix is complex symmetric: G(d) = G(d)^T = G(-d) (greens.rs:34-71), the
+// FCD cell average is symmetric in its two dipoles (greens.rs:94-167: the
+// 27 nodes are symmetric about the cell centre), and the diagonal blocks
+// sit in diagonal tiles, which are stored whole.  So A is kept as its tiles
+// (I, J), I <= J, of kSymTile x kSymTile entries -- half the bytes of the
+// dense rows -- and a product reads each stored tile once and applies it
+// twice: y_I += A_IJ x_J (row side) and, for I < J, y_J += A_IJ^T x_I
+// (column side).
+// ---------------------------------------------------------------------------
+constexpr int kSymTileDip = kSymTile / 3;         // 64 dipoles a side
+constexpr int kSymWarps = 8;
+constexpr int kSymRowsPerWarp = kSymTile / kSymWarps;  // 24
+
+// Offset (in tiles) of tile (I, J), I <= J, among nt tiles a side: the
+// tile rows before I hold sum_{r < I} (nt - r) = I (2 nt - I + 1) / 2 tiles.
+__host__ __device__ __forceinline__ size_t sym_tile_offset(int I, int J, int nt) {
+  return (size_t)I * (size_t)(2 * nt - I + 1) / 2 + (size_t)(J - I);
+}
+
+// One block per tile (I, J) of the grid (nt, nt); blocks below the diagonal
+// return.  Each thread evaluates whole 3x3 dipole blocks (i, j) as
+// assemble_pairs does for a free-space system: alpha^-1 on i == j, -G_ij
+// otherwise.  Entries past dim keep the zero of the allocation.
+template <typename T2>
+__global__ void __launch_bounds__(256)
+assemble_sym_tiles(int n, int nt, const double4* __restrict__ pos,
+                   const double2* __restrict__ inv_alpha, double k, T2* __restrict__ A) {
+  const int I = blockIdx.y, J = blockIdx.x;
+  if (I > J) return;
+  T2* tile = A + sym_tile_offset(I, J, nt) * (size_t)(kSymTile * kSymTile);
+  for (int q = threadIdx.x; q < kSymTileDip * kSymTileDip; q += blockDim.x) {
+    const int li = q / kSymTileDip, lj = q % kSymTileDip;
+    const int i = I * kSymTileDip + li, j = J * kSymTileDip + lj;
+    if (i >= n || j >= n) continue;
+    double2 blk[9];
+    if (i == j) {
+      for (int e = 0; e < 9; ++e) blk[e] = inv_alpha[(size_t)e * n + i];
+    } else {
+      const double4 ri = pos[i], rj = pos[j];
+      double2 g[9];
+      greens_point_d(ri.x - rj.x, ri.y - rj.y, ri.z - rj.z, k, g);
+      for (int e = 0; e < 9; ++e) blk[e] = make_double2(-g[e].x, -g[e].y);
+    }
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b)
+        tile[(size_t)(3 * li + a) * kSymTile + 3 * lj + b] =
+            mk<T2>(blk[3 * a + b].x, blk[3 * a + b].y);
+  }
+}
+
+// FCD: A[i][j] -= (G_fcd - G_point) for the near pairs whose block is
+// stored (tile of i <= tile of j); the pair (j, i) of the other tiles is the
+// transpose and is read through the column side of the product.
+template <typename T2>
+__global__ void assemble_sym_fcd(int n, int nt, int ell_w, const int* __restrict__ near_j,
+                                 const double2* __restrict__ fcd, T2* __restrict__ A) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n * ell_w) return;
+  const int w = idx / n, i = idx % n;
+  const int j = near_j[(size_t)w * n + i];
+  if (j < 0) return;
+  const int I = i / kSymTileDip, J = j / kSymTileDip;
+  if (I > J) return;
+  T2* tile = A + sym_tile_offset(I, J, nt) * (size_t)(kSymTile * kSymTile);
+  const int li = i - I * kSymTileDip, lj = j - J * kSymTileDip;
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) {
+      const double2 c = fcd[((size_t)w * 9 + 3 * a + b) * n + i];
+      T2& e = tile[(size_t)(3 * li + a) * kSymTile + 3 * lj + b];
+      e = mk<T2>((double)e.x - c.x, (double)e.y - c.y);
+    }
+}
+
+// Element types of the tile product: FP32 storage computes in FP32 (as the
+// FP32 operator does), FP64 storage in FP64; a 16-byte load carries CPV
+// complex entries.
+template <typename T2> struct SymGemvT;
+template <> struct SymGemvT<float2> {
+  using R = float;
+  using V = float4;
+  static constexpr int CPV = 2;
+  static constexpr int RG = 4;  // rows whose loads are in flight together
+  __device__ static float2 get(const float4& v, int h) {
+    return h == 0 ? make_float2(v.x, v.y) : make_float2(v.z, v.w);
+  }
+};
+template <> struct SymGemvT<double2> {
+  using R = double;
+  using V = double2;
+  static constexpr int CPV = 1;
+  static constexpr int RG = 2;
+  __device__ static double2 get(const double2& v, int) { return v; }
+};
+
+// Sum over the 32 lanes of 16 values per lane, transposed: afterwards lane l
+// holds in v[0] the total of value 8 b4 + 4 b3 + 2 b2 + b1 (b = bits of l);
+// lanes l and l ^ 1 hold the same total.
+template <typename R>
+__device__ __forceinline__ void sym_transpose_reduce16(R (&v)[16], int lane) {
+#pragma unroll
+  for (int h = 8, m = 16; h >= 1; h >>= 1, m >>= 1) {
+    const bool up = (lane & m) != 0;
+#pragma unroll
+    for (int i = 0; i < h; ++i) {
+      const R send = up ? v[i] : v[i + h];
+      const R keep = up ? v[i + h] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, m);
+    }
+  }
+  v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
+}
+
+// One block per stored tile (items[blockIdx.x] = (I, J)).  Warp w owns tile
+// rows 24 w .. 24 w + 23; lane l owns the complex columns CPV (l + 32 e) + h
+// (e < 6 / CPV, h < CPV), so every load instruction of a warp reads one
+// contiguous run of a tile row.  Row side: each row's 6 products per lane
+// are summed over the warp by a transposed shuffle reduction, 8 rows at a
+// time.  Column side: each lane sums A[r][c] x_I[r] over its warp's rows,
+// and the 8 warps' sums are added in warp order through shared memory.
+// Output (no atomics, every entry written once per product):
+//   part[J][I*T + r] = sum_c A_IJ[r][c] x_J[c]       (row side)
+//   part[I][J*T + c] = sum_r A_IJ[r][c] x_I[r]       (column side, I < J)
+// so for the rows of tile row R, slot S >= R comes from tile (R, S) and slot
+// S < R from tile (S, R); gemv_reduce adds the nt slots in order.
+template <typename T2>
+__global__ void __launch_bounds__(kSymWarps * 32, 2)
+gemv_sym_tiles(int dim, int nt, const T2* __restrict__ A, const int2* __restrict__ items,
+               const double2* __restrict__ x, double2* __restrict__ part,
+               const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  using G = SymGemvT<T2>;
+  using R = typename G::R;
+  using V = typename G::V;
+  constexpr int CPV = G::CPV, RG = G::RG;
+  constexpr int EV = kSymTile / (32 * CPV);  // 16-byte loads per lane per row
+  constexpr int VPR = kSymTile / CPV;        // 16-byte vectors per tile row
+  __shared__ R sXI[2 * kSymTile];            // x_I (re, im), zero past dim
+  __shared__ R sCol[kSymWarps][2 * kSymTile];
+  const int2 it = items[blockIdx.x];
+  const int I = it.x, J = it.y;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int rowI0 = I * kSymTile, colJ0 = J * kSymTile;
+  if (tid < kSymTile) {
+    const int r = rowI0 + tid;
+    const double2 v = r < dim ? x[r] : make_double2(0.0, 0.0);
+    sXI[2 * tid] = (R)v.x;
+    sXI[2 * tid + 1] = (R)v.y;
+  }
+  // x_J at this lane's columns
+  R xr[EV * CPV], xi[EV * CPV];
+#pragma unroll
+  for (int e = 0; e < EV; ++e)
+#pragma unroll
+    for (int h = 0; h < CPV; ++h) {
+      const int c = colJ0 + CPV * (lane + 32 * e) + h;
+      const double2 v = c < dim ? x[c] : make_double2(0.0, 0.0);
+      xr[e * CPV + h] = (R)v.x;
+      xi[e * CPV + h] = (R)v.y;
+    }
+  __syncthreads();
+  R cr[EV * CPV], ci[EV * CPV];
+#pragma unroll
+  for (int q = 0; q < EV * CPV; ++q) cr[q] = ci[q] = (R)0;
+  const bool offdiag = I != J;
+  const V* tile = reinterpret_cast<const V*>(A + sym_tile_offset(I, J, nt) *
+                                                     (size_t)(kSymTile * kSymTile));
+  const int r_begin = warp * kSymRowsPerWarp;
+  double2* slotJ = part + (size_t)J * dim;  // row side of this tile
+#pragma unroll 1
+  for (int g8 = 0; g8 < kSymRowsPerWarp; g8 += 8) {
+    R red[16];
+#pragma unroll
+    for (int k0 = 0; k0 < 8; k0 += RG) {
+      V v[RG][EV];
+#pragma unroll
+      for (int k = 0; k < RG; ++k)
+#pragma unroll
+        for (int e = 0; e < EV; ++e)
+          v[k][e] = __ldcs(&tile[(size_t)(r_begin + g8 + k0 + k) * VPR + lane + 32 * e]);
+#pragma unroll
+      for (int k = 0; k < RG; ++k) {
+        const int lr = r_begin + g8 + k0 + k;
+        const R ar = sXI[2 * lr], ai = sXI[2 * lr + 1];
+        R sr = (R)0, si = (R)0;
+#pragma unroll
+        for (int e = 0; e < EV; ++e)
+#pragma unroll
+          for (int h = 0; h < CPV; ++h) {
+            const T2 a = G::get(v[k][e], h);
+            const int q = e * CPV + h;
+            sr += (R)a.x * xr[q] - (R)a.y * xi[q];
+            si += (R)a.x * xi[q] + (R)a.y * xr[q];
+            cr[q] += (R)a.x * ar - (R)a.y * ai;
+            ci[q] += (R)a.x * ai + (R)a.y * ar;
+          }
+        red[2 * (k0 + k)] = sr;
+        red[2 * (k0 + k) + 1] = si;
+      }
+    }
+    sym_transpose_reduce16(red, lane);
+    if ((lane & 1) == 0) {
+      const int vidx = 8 * ((lane >> 4) & 1) + 4 * ((lane >> 3) & 1) + 2 * ((lane >> 2) & 1) +
+                       ((lane >> 1) & 1);
+      const int row = rowI0 + r_begin + g8 + (vidx >> 1);
+      if (row < dim) reinterpret_cast<double*>(slotJ + row)[vidx & 1] = (double)red[0];
+    }
+  }
+  if (!offdiag) return;  // a diagonal tile is stored whole: no column side
+#pragma unroll
+  for (int e = 0; e < EV; ++e)
+#pragma unroll
+    for (int h = 0; h < CPV; ++h) {
+      const int c = CPV * (lane + 32 * e) + h, q = e * CPV + h;
+      sCol[warp][2 * c] = cr[q];
+      sCol[warp][2 * c + 1] = ci[q];
+    }
+  __syncthreads();
+  if (tid < kSymTile) {
+    const int row = colJ0 + tid;
+    if (row < dim) {
+      double sr = 0.0, si = 0.0;
+#pragma unroll
+      for (int w = 0; w < kSymWarps; ++w) {
+        sr += (double)sCol[w][2 * tid];
+        si += (double)sCol[w][2 * tid + 1];
+      }
+      part[(size_t)I * dim + row] = make_double2(sr, si);
+    }
+  }
+}
+
 // y = A x in two launches.  gemv_part: one warp per (row, column chunk), the
 // chunk streamed with 16-byte loads (two FP32 complex or one FP64 complex per
 // load, four in flight per lane), FP64 accumulation, shuffle reduction, one
@@ -239,9 +472,34 @@ __global__ void narrow_rows(size_t rows, int dim, const double2* __restrict__ sr
   }
 }
 
-lum_status CachedOperator::allocate(int dim_, int precision_) {
+lum_status CachedOperator::allocate(int dim_, int precision_, bool packed_) {
   dim = dim_;
   precision = precision_;
+  packed = packed_;
+  if (packed) {
+    if (dim % 3 != 0) {
+      set_error("symmetric tile storage needs whole 3x3 dipole blocks (dim %d)", dim);
+      return LUM_ERR_INVALID;
+    }
+    nt = (dim + kSymTile - 1) / kSymTile;
+    const size_t tiles = (size_t)nt * (nt + 1) / 2;
+    const size_t es = (precision == LUM_FP32) ? sizeof(float2) : sizeof(double2);
+    ld = 0;
+    LUM_TRY(A.alloc(es * tiles * kSymTile * kSymTile));
+    LUM_TRY_CUDA(cudaMemset(A.p, 0, A.bytes));
+    std::vector<int2> it;
+    it.reserve(tiles);
+    for (int I = 0; I < nt; ++I)
+      for (int J = I; J < nt; ++J) it.push_back(make_int2(I, J));
+    LUM_TRY(sym_items.alloc(sizeof(int2) * tiles));
+    LUM_TRY_CUDA(cudaMemcpy(sym_items.p, it.data(), sizeof(int2) * tiles,
+                            cudaMemcpyHostToDevice));
+    LUM_TRY(sym_part.alloc(sizeof(double2) * (size_t)nt * dim));
+    tc.release();
+    gemv_chunks = 0;
+    return LUM_OK;
+  }
+  nt = 0;
   // Rows are padded to a multiple of 16 complex entries (128 B in FP32):
   // every row starts 128-byte aligned, and the tensor-core GEMM reads the
   // matrix through a TMA map whose row pitch must be a multiple of 16 bytes.
@@ -281,6 +539,38 @@ lum_status CachedOperator::upload(const double* host, cudaStream_t st) {
 
 lum_status CachedOperator::assemble(const OtfOperator& g, cudaStream_t st) {
   const int n = g.n;
+  if (packed) {
+    if (g.has_lattice || g.has_substrate || g.has_somm) {
+      set_error("symmetric tile storage needs a free-space system (no lattice sum, no "
+                "substrate)");
+      return LUM_ERR_INVALID;
+    }
+    if (3 * n != dim) {
+      set_error("symmetric tile storage of dimension %d for %d dipoles", dim, n);
+      return LUM_ERR_INVALID;
+    }
+    const dim3 grid(nt, nt);
+    if (precision == LUM_FP32)
+      assemble_sym_tiles<float2><<<grid, 256, 0, st>>>(n, nt, g.pos64.as<double4>(),
+                                                       g.inv_alpha.as<double2>(), g.k,
+                                                       A.as<float2>());
+    else
+      assemble_sym_tiles<double2><<<grid, 256, 0, st>>>(n, nt, g.pos64.as<double4>(),
+                                                        g.inv_alpha.as<double2>(), g.k,
+                                                        A.as<double2>());
+    LUM_CHECK_LAUNCH();
+    if (g.ell_w > 0) {
+      const int total = n * g.ell_w;
+      if (precision == LUM_FP32)
+        assemble_sym_fcd<float2><<<(total + 255) / 256, 256, 0, st>>>(
+            n, nt, g.ell_w, g.near_j.as<int>(), g.fcd64.as<double2>(), A.as<float2>());
+      else
+        assemble_sym_fcd<double2><<<(total + 255) / 256, 256, 0, st>>>(
+            n, nt, g.ell_w, g.near_j.as<int>(), g.fcd64.as<double2>(), A.as<double2>());
+      LUM_CHECK_LAUNCH();
+    }
+    return LUM_OK;
+  }
   const long long npairs = (long long)n * n;
   const int threads = 128;
   const long long blocks = (npairs + threads - 1) / threads;
@@ -318,6 +608,19 @@ lum_status CachedOperator::assemble(const OtfOperator& g, cudaStream_t st) {
 
 lum_status CachedOperator::apply(const double2* x, double2* y, cudaStream_t st,
                                  const int* skip) {
+  if (packed) {
+    const unsigned tiles = (unsigned)((size_t)nt * (nt + 1) / 2);
+    if (precision == LUM_FP32)
+      gemv_sym_tiles<float2><<<tiles, kSymWarps * 32, 0, st>>>(
+          dim, nt, A.as<float2>(), sym_items.as<int2>(), x, sym_part.as<double2>(), skip);
+    else
+      gemv_sym_tiles<double2><<<tiles, kSymWarps * 32, 0, st>>>(
+          dim, nt, A.as<double2>(), sym_items.as<int2>(), x, sym_part.as<double2>(), skip);
+    LUM_CHECK_LAUNCH();
+    gemv_reduce<<<(dim + 255) / 256, 256, 0, st>>>(dim, nt, sym_part.as<double2>(), y, skip);
+    LUM_CHECK_LAUNCH();
+    return LUM_OK;
+  }
   if (gemv_chunks == 0) {
     // about 8 waves of 8-warp blocks (8 resident per SM), chunks of >= 512
     // complex entries, an even chunk length (16-byte loads of FP32 pairs)
@@ -376,6 +679,20 @@ lum_status CachedOperator::apply_multi_cuda_cores(const double2* X, double2* Y, 
 
 lum_status CachedOperator::apply_multi(const double2* X, double2* Y, int nrhs, long long sc,
                                        long long sr, int method, cudaStream_t st) {
+  if (packed) {
+    // one tile product per vector; the tensor-core product reads dense rows
+    if (method == LUM_MATMUL_TENSOR) {
+      set_error("the tensor-core product needs dense matrix storage, not symmetric tiles");
+      return LUM_ERR_INVALID;
+    }
+    if (sc != 1) {
+      set_error("a symmetric-tile matrix takes its vectors back to back (one vector, or "
+                "lum_session_matmul_vectors)");
+      return LUM_ERR_INVALID;
+    }
+    for (int r = 0; r < nrhs; ++r) LUM_TRY(apply(X + r * sr, Y + r * sr, st));
+    return LUM_OK;
+  }
   const bool tensor = precision == LUM_FP32 &&
                       (method == LUM_MATMUL_TENSOR || (method == LUM_MATMUL_AUTO && nrhs >= kTcMinRhs));
   if (method == LUM_MATMUL_TENSOR && precision != LUM_FP32) {

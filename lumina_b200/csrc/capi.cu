@@ -499,6 +499,10 @@ int lum_session_set_wavelength(lum_session* s, double k, const double* inv_alpha
     set_error("a Sommerfeld session takes no Fresnel substrate");
     return LUM_ERR_INVALID;
   }
+  if (s->kind == 1 && s->cached.packed && substrate) {
+    set_error("symmetric tile storage needs a free-space system (no substrate)");
+    return LUM_ERR_INVALID;
+  }
   cudaSetDevice(s->ctx->device);
   LUM_TRY(s->otf.set_physics(k, inv_alpha, s->otf.use_fcd, s->otf.cell, nullptr, nullptr,
                              substrate, s->stream));
@@ -535,8 +539,15 @@ int lum_session_assemble(lum_ctx* ctx, int n, const double* pos, const double* i
   if (bad_ptr(ctx, "ctx") || bad_ptr(out, "out")) return LUM_ERR_INVALID;
   *out = nullptr;
   LUM_TRY(check_inputs(n, pos, inv_alpha, k));
+  const bool sym = (precision & LUM_STORAGE_SYMMETRIC) != 0;
+  precision &= ~LUM_STORAGE_SYMMETRIC;
   if (precision != LUM_FP32 && precision != LUM_FP64) {
     set_error("invalid storage precision %d", precision);
+    return LUM_ERR_INVALID;
+  }
+  if (sym && (lattice || substrate)) {
+    set_error("symmetric tile storage needs a free-space system (no lattice sum, no "
+              "substrate)");
     return LUM_ERR_INVALID;
   }
   lum_session* s = nullptr;
@@ -544,7 +555,7 @@ int lum_session_assemble(lum_ctx* ctx, int n, const double* pos, const double* i
   lum_status st = s->otf.build_geometry(pos, n, s->stream);
   if (st == LUM_OK)
     st = s->otf.set_physics(k, inv_alpha, use_fcd, cell, lattice, k_bloch, substrate, s->stream);
-  if (st == LUM_OK) st = s->cached.allocate(3 * n, precision);
+  if (st == LUM_OK) st = s->cached.allocate(3 * n, precision, sym);
   if (st == LUM_OK) st = s->cached.assemble(s->otf, s->stream);
   if (st == LUM_OK) {
     cudaError_t e = cudaStreamSynchronize(s->stream);
@@ -618,6 +629,10 @@ int lum_session_assemble_sommerfeld(lum_ctx* ctx, int n, const double* pos,
 
 int lum_session_set_sommerfeld(lum_session* s, const lum_sommerfeld* somm) {
   if (bad_ptr(s, "session") || bad_ptr(somm, "somm")) return LUM_ERR_INVALID;
+  if (s->kind == 1 && s->cached.packed) {
+    set_error("symmetric tile storage needs a free-space system (no substrate)");
+    return LUM_ERR_INVALID;
+  }
   if (s->kind == 2) {
     if (s->fft.refl_mode == 1) {
       set_error("the session already has a Fresnel substrate");

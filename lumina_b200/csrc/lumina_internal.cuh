@@ -236,6 +236,11 @@ struct TcWork {
 // Right-hand sides from which the automatic method takes the tensor cores.
 constexpr int kTcMinRhs = 4;
 
+// Symmetric tile storage of a cached matrix: tiles of kSymTile x kSymTile
+// complex entries (kSymTile / 3 dipoles a side, so no 3x3 dipole block
+// straddles two tiles); only the tiles (I, J) with I <= J are stored.
+constexpr int kSymTile = 192;
+
 struct CachedOperator {
   int dim = 0;              // 3N
   size_t ld = 0;            // row pitch in complex entries (dim rounded up to 16)
@@ -245,7 +250,13 @@ struct CachedOperator {
   int gemv_chunks = 0;      // column chunks of the GEMV (0: not yet chosen)
   int gemv_chunk = 0;       // complex entries per chunk
   DevBuf gemv_part_buf;     // double2 [gemv_chunks][dim] per-chunk partial sums
-  lum_status allocate(int dim, int precision);
+  // Symmetric tile storage (A = A^T): A holds the upper-triangle tiles,
+  // packed row by row, each tile row-major with zero padding past dim.
+  bool packed = false;
+  int nt = 0;               // tiles per side, ceil(dim / kSymTile)
+  DevBuf sym_items;         // int2 (I, J) per stored tile
+  DevBuf sym_part;          // double2 [nt][dim]: slot S, row r (see cached.cu)
+  lum_status allocate(int dim, int precision, bool packed = false);
   lum_status upload(const double* host, cudaStream_t st);
   lum_status assemble(const OtfOperator& geo, cudaStream_t st);
   lum_status apply(const double2* x, double2* y, cudaStream_t st, const int* skip = nullptr);
