@@ -416,6 +416,10 @@ int lum_session_upload_matrix(lum_session* s, const double* A) {
     set_error("upload_matrix needs a cached session");
     return LUM_ERR_INVALID;
   }
+  if (s->cached.packed) {
+    set_error("upload_matrix takes dense rows; this session keeps symmetric tiles");
+    return LUM_ERR_INVALID;
+  }
   cudaSetDevice(s->ctx->device);
   return s->cached.upload(A, s->stream);
 }

@@ -145,6 +145,8 @@ def test_sym_tiles_vectors_and_rhs_batch(backend, rng):
         Ya = s.matmul(X, "auto")
         with pytest.raises(InvalidGeometry):
             s.matmul(X, "tensor")
+        with pytest.raises(InvalidGeometry):  # dense rows cannot be uploaded into tiles
+            s.upload_matrix(A)
         B = s.rhs_batch(len(rhs))
         xb, info = B.solve(np.concatenate(rhs), 1e-10, 5000, 30, "fp64")
         B.close()
