@@ -9,7 +9,11 @@ cross sections) and the dispatch of :238-419 with every branch on the device:
   and solved by device GMRES to ``direct_tolerance`` (default 1e-12), which
   agrees with an LU solve to ~1e-12 relative.
 * matrix within matrix_memory_budget: device assembly (FCD, lattice and
-  substrate terms included) + device GMRES on the cached matrix.
+  substrate terms included) + device GMRES on the cached matrix.  A
+  free-space matrix (no lattice, no substrate) is complex symmetric and is
+  kept as its upper-triangle tiles (``symmetric_storage``, default on): half
+  the memory and half the bytes per product; the budget test stays the
+  reference's (3N)^2 * 16 bytes, so the branch choice is unchanged.
 * otherwise: the matrix-free on-the-fly session + device GMRES.
 
 Before the cached / on-the-fly branches, like the reference's FFT branch
@@ -62,6 +66,7 @@ class CdaSolver:
     restart: int = 30
     use_fft: bool = True
     reuse_session: bool = True
+    symmetric_storage: bool = True
 
     def __post_init__(self):
         if self.backend is None:
@@ -122,6 +127,9 @@ class CdaSolver:
         elif direct or (3 * n) ** 2 * 16 <= self.matrix_memory_budget:
             branch = "cached"
             storage = "fp32" if (self.precision == "fp32_refine" and not direct) else "fp64"
+            # a free-space matrix is complex symmetric: keep its upper tiles only
+            if self.symmetric_storage and self.lattice is None and sub is None:
+                storage += "+sym"
         else:
             branch = "onthefly"
         pos = np.ascontiguousarray(np.asarray(dipoles.positions, np.float64))
@@ -141,7 +149,8 @@ class CdaSolver:
         if branch == "cached":
             return self.backend.assemble_and_create_session(
                 dipoles.positions, k, inv_alpha, use_fcd=self.use_fcd, cell_size=self.cell_size,
-                lattice=self.lattice, k_bloch=params.k_bloch, substrate=sub, precision=storage)
+                lattice=self.lattice, k_bloch=params.k_bloch, substrate=sub,
+                precision=storage.split("+")[0], symmetric=storage.endswith("+sym"))
         return self.backend.create_onthefly_session(
             dipoles.positions, inv_alpha, k, use_fcd=self.use_fcd, cell_size=self.cell_size,
             lattice=self.lattice, k_bloch=params.k_bloch, substrate=sub)

@@ -168,3 +168,32 @@ def test_sym_tiles_reject_lattice_and_substrate(backend):
     with pytest.raises(InvalidGeometry):
         backend.assemble_and_create_session(w.positions, w.k, inv, True, 2.0, lattice=lat,
                                             symmetric=True)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32_refine"])
+def test_cdasolver_cached_branch_keeps_symmetric_tiles(backend, precision):
+    """CdaSolver's cached branch (cda/mod.rs:346-374) keeps a free-space
+    matrix as symmetric tiles; cross sections equal those over dense rows,
+    and a substrate system on the same solver falls back to dense rows."""
+    from lumina_b200.lattice import SubstrateRuntime as Sub
+    w = configs.sphere_au_925()
+    kw = dict(iterative_threshold=0, cell_size=2.0, matrix_memory_budget=2 << 30,
+              precision=precision)
+    sym = lb.CdaSolver(backend=backend, **kw)
+    dense = lb.CdaSolver(backend=backend, symmetric_storage=False, **kw)
+    ds = lb.DipoleSet(w.positions, w.alpha)
+    params = lb.SimulationParams(solver_tolerance=1e-10, max_iterations=20000)
+    a = sym.compute_cross_sections(ds, 520.0, params)
+    assert sym._kept[0][0] == "cached" and sym._kept[0][1].endswith("+sym")
+    b = dense.compute_cross_sections(ds, 520.0, params)
+    assert not dense._kept[0][1].endswith("+sym")
+    assert abs(a.extinction - b.extinction) <= 1e-8 * abs(b.extinction)
+    assert abs(a.absorption - b.absorption) <= 1e-8 * abs(b.absorption)
+    pos = w.positions + np.array([0.0, 0.0, 20.0])
+    ds2 = lb.DipoleSet(pos, w.alpha)
+    p2 = lb.SimulationParams(solver_tolerance=1e-10, max_iterations=20000,
+                             substrate_runtime=Sub(0.0, complex(0.45 / 2.45)))
+    c = sym.compute_cross_sections(ds2, 520.0, p2)
+    assert sym._kept[0][1] in ("fp64", "fp32") and c.extinction > 0
+    sym.close()
+    dense.close()
