@@ -900,7 +900,7 @@ def _bench_cached(args, bk, stream, torch, lb, configs):
     torch.cuda.synchronize()
     sym_diff = float(torch.max(torch.abs(y_sym - y_dense)) / torch.max(torch.abs(y_dense)))
     Ssym.close()
-    tile = 192
+    tile = 192  # the library's tile side (kSymTile, 64 dipoles)
     nt = -(-dim // tile)
     sym_bytes = 8.0 * tile * tile * nt * (nt + 1) / 2   # stored tiles, zero padding included
     slot_bytes = 2.0 * 16.0 * nt * dim                  # per-tile partials written and summed
