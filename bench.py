@@ -928,7 +928,10 @@ def _bench_cached(args, bk, stream, torch, lb, configs):
                        "n_dipoles": n, "dim": dim, "matrix_gb": a_bytes / 1e9, "nrhs": R,
                        "l2": "256 MB flush before each timed product; matrix >> L2"},
             "assemble_s": assemble_s,
-            "roofline": {"bound": "hbm", "kernel": "gemv_part<float2> + gemv_reduce",
+            "roofline": {"bound": "hbm",
+                         "kernel": ("gemv_part<float2> + gemv_reduce"
+                                    if os.environ.get("LUMINA_DENSE_GEMV") == "rows" else
+                                    "gemv_sym_tiles<float2, dense rows> + gemv_reduce"),
                          "achieved": a_bytes / (ms_gemv * 1e-3) / 1e9, "peak": hbm_peak,
                          "unit": "GB/s", "frac": a_bytes / (ms_gemv * 1e-3) / 1e9 / hbm_peak,
                          "traffic": None, "peak_source": hbm_src},

@@ -11,11 +11,18 @@
 // included as in the reference.
 //
 // Matvec (MatvecSession::matvec): y = A x is bound by reading A from HBM
-// (8 or 16 bytes per complex entry).  One warp per row streams the row with
-// coalesced 8/16-byte loads, x is read through L1/L2 (3N complex is a few
-// MB at most), products accumulate in FP64 and the warp reduces by shuffle.
+// (8 or 16 bytes per complex entry).  The product runs over blocks of
+// 192 x 192 entries (gemv_sym_tiles): one CTA reads a block once with
+// 16-byte streaming loads, holds the block's 192 entries of x in registers
+// and shared memory, and writes the block's partial row sums to a slot that
+// gemv_reduce adds in order.  The same kernel serves the symmetric tile
+// storage, where each stored tile is also applied transposed.  The older
+// row-chunk GEMV (gemv_part: one warp per row chunk, FP64 accumulation) is
+// kept behind LUMINA_DENSE_GEMV=rows.
 #include "lumina_internal.cuh"
 #include "device_physics.cuh"
+
+#include <cstdlib>
 
 namespace lum {
 
@@ -224,20 +231,27 @@ __device__ __forceinline__ void sym_transpose_reduce16(R (&v)[16], int lane) {
 //   part[I][J*T + c] = sum_r A_IJ[r][c] x_I[r]       (column side, I < J)
 // so for the rows of tile row R, slot S >= R comes from tile (R, S) and slot
 // S < R from tile (S, R); gemv_reduce adds the nt slots in order.
-template <typename T2>
+//
+// DENSE: the same row side over dense rows [dim][ld] (every block (I, J) of
+// the nt x nt grid, no column side): the block of rows I*T.. and columns
+// J*T.. is read with the row pitch ld, rows past dim and vectors past ld
+// are not read.  Against gemv_part (a warp streaming one row chunk, FP64
+// accumulation) it keeps x_J in registers for all 192 rows of the block and
+// computes FP32 storage in FP32, so no x is re-read per row and no FP32
+// entry is converted to FP64.
+template <typename T2, bool DENSE>
 __global__ void __launch_bounds__(kSymWarps * 32, 2)
-gemv_sym_tiles(int dim, int nt, const T2* __restrict__ A, const int2* __restrict__ items,
-               const double2* __restrict__ x, double2* __restrict__ part,
-               const int* __restrict__ skip) {
+gemv_sym_tiles(int dim, int nt, size_t ld, const T2* __restrict__ A,
+               const int2* __restrict__ items, const double2* __restrict__ x,
+               double2* __restrict__ part, const int* __restrict__ skip) {
   if (skip && *skip) return;
   using G = SymGemvT<T2>;
   using R = typename G::R;
   using V = typename G::V;
   constexpr int CPV = G::CPV, RG = G::RG;
   constexpr int EV = kSymTile / (32 * CPV);  // 16-byte loads per lane per row
-  constexpr int VPR = kSymTile / CPV;        // 16-byte vectors per tile row
   __shared__ R sXI[2 * kSymTile];            // x_I (re, im), zero past dim
-  __shared__ R sCol[kSymWarps][2 * kSymTile];
+  __shared__ R sCol[DENSE ? 1 : kSymWarps][2 * kSymTile];
   const int2 it = items[blockIdx.x];
   const int I = it.x, J = it.y;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -263,9 +277,18 @@ gemv_sym_tiles(int dim, int nt, const T2* __restrict__ A, const int2* __restrict
   R cr[EV * CPV], ci[EV * CPV];
 #pragma unroll
   for (int q = 0; q < EV * CPV; ++q) cr[q] = ci[q] = (R)0;
-  const bool offdiag = I != J;
-  const V* tile = reinterpret_cast<const V*>(A + sym_tile_offset(I, J, nt) *
-                                                     (size_t)(kSymTile * kSymTile));
+  const bool offdiag = !DENSE && I != J;
+  // the block's first vector and the row pitch in 16-byte vectors
+  const V* tile = DENSE ? reinterpret_cast<const V*>(A + (size_t)rowI0 * ld + colJ0)
+                        : reinterpret_cast<const V*>(A + sym_tile_offset(I, J, nt) *
+                                                             (size_t)(kSymTile * kSymTile));
+  const size_t pitch = DENSE ? ld / CPV : (size_t)(kSymTile / CPV);
+  // DENSE: this lane's vectors that lie inside the row pitch (ld is a
+  // multiple of 16 complex entries, so a vector is inside or past it whole)
+  bool vec_ok[EV];
+#pragma unroll
+  for (int e = 0; e < EV; ++e)
+    vec_ok[e] = !DENSE || (size_t)colJ0 + (size_t)(CPV * (lane + 32 * e)) < ld;
   const int r_begin = warp * kSymRowsPerWarp;
   double2* slotJ = part + (size_t)J * dim;  // row side of this tile
 #pragma unroll 1
@@ -275,10 +298,14 @@ gemv_sym_tiles(int dim, int nt, const T2* __restrict__ A, const int2* __restrict
     for (int k0 = 0; k0 < 8; k0 += RG) {
       V v[RG][EV];
 #pragma unroll
-      for (int k = 0; k < RG; ++k)
+      for (int k = 0; k < RG; ++k) {
+        const int lr = r_begin + g8 + k0 + k;
+        const bool row_ok = !DENSE || rowI0 + lr < dim;
 #pragma unroll
         for (int e = 0; e < EV; ++e)
-          v[k][e] = __ldcs(&tile[(size_t)(r_begin + g8 + k0 + k) * VPR + lane + 32 * e]);
+          v[k][e] = (row_ok && vec_ok[e]) ? __ldcs(&tile[(size_t)lr * pitch + lane + 32 * e])
+                                          : V{};
+      }
 #pragma unroll
       for (int k = 0; k < RG; ++k) {
         const int lr = r_begin + g8 + k0 + k;
@@ -307,26 +334,29 @@ gemv_sym_tiles(int dim, int nt, const T2* __restrict__ A, const int2* __restrict
       if (row < dim) reinterpret_cast<double*>(slotJ + row)[vidx & 1] = (double)red[0];
     }
   }
-  if (!offdiag) return;  // a diagonal tile is stored whole: no column side
+  // a diagonal tile is stored whole, and dense rows have no column side
+  if constexpr (!DENSE) {
+    if (!offdiag) return;
 #pragma unroll
-  for (int e = 0; e < EV; ++e)
+    for (int e = 0; e < EV; ++e)
 #pragma unroll
-    for (int h = 0; h < CPV; ++h) {
-      const int c = CPV * (lane + 32 * e) + h, q = e * CPV + h;
-      sCol[warp][2 * c] = cr[q];
-      sCol[warp][2 * c + 1] = ci[q];
-    }
-  __syncthreads();
-  if (tid < kSymTile) {
-    const int row = colJ0 + tid;
-    if (row < dim) {
-      double sr = 0.0, si = 0.0;
-#pragma unroll
-      for (int w = 0; w < kSymWarps; ++w) {
-        sr += (double)sCol[w][2 * tid];
-        si += (double)sCol[w][2 * tid + 1];
+      for (int h = 0; h < CPV; ++h) {
+        const int c = CPV * (lane + 32 * e) + h, q = e * CPV + h;
+        sCol[warp][2 * c] = cr[q];
+        sCol[warp][2 * c + 1] = ci[q];
       }
-      part[(size_t)I * dim + row] = make_double2(sr, si);
+    __syncthreads();
+    if (tid < kSymTile) {
+      const int row = colJ0 + tid;
+      if (row < dim) {
+        double sr = 0.0, si = 0.0;
+#pragma unroll
+        for (int w = 0; w < kSymWarps; ++w) {
+          sr += (double)sCol[w][2 * tid];
+          si += (double)sCol[w][2 * tid + 1];
+        }
+        part[(size_t)I * dim + row] = make_double2(sr, si);
+      }
     }
   }
 }
@@ -472,6 +502,20 @@ __global__ void narrow_rows(size_t rows, int dim, const double2* __restrict__ sr
   }
 }
 
+// The work list of a tile product and its per-block partial sums: the
+// stored tiles I <= J (symmetric storage) or every block (I, J) of the
+// nt x nt grid (dense rows).
+lum_status CachedOperator::tile_blocks(bool upper) {
+  std::vector<int2> it;
+  for (int I = 0; I < nt; ++I)
+    for (int J = upper ? I : 0; J < nt; ++J) it.push_back(make_int2(I, J));
+  LUM_TRY(tile_items.alloc(sizeof(int2) * it.size()));
+  LUM_TRY_CUDA(cudaMemcpy(tile_items.p, it.data(), sizeof(int2) * it.size(),
+                          cudaMemcpyHostToDevice));
+  LUM_TRY(tile_part.alloc(sizeof(double2) * (size_t)nt * dim));
+  return LUM_OK;
+}
+
 lum_status CachedOperator::allocate(int dim_, int precision_, bool packed_) {
   dim = dim_;
   precision = precision_;
@@ -487,19 +531,14 @@ lum_status CachedOperator::allocate(int dim_, int precision_, bool packed_) {
     ld = 0;
     LUM_TRY(A.alloc(es * tiles * kSymTile * kSymTile));
     LUM_TRY_CUDA(cudaMemset(A.p, 0, A.bytes));
-    std::vector<int2> it;
-    it.reserve(tiles);
-    for (int I = 0; I < nt; ++I)
-      for (int J = I; J < nt; ++J) it.push_back(make_int2(I, J));
-    LUM_TRY(sym_items.alloc(sizeof(int2) * tiles));
-    LUM_TRY_CUDA(cudaMemcpy(sym_items.p, it.data(), sizeof(int2) * tiles,
-                            cudaMemcpyHostToDevice));
-    LUM_TRY(sym_part.alloc(sizeof(double2) * (size_t)nt * dim));
+    LUM_TRY(tile_blocks(true));
     tc.release();
     gemv_chunks = 0;
     return LUM_OK;
   }
-  nt = 0;
+  nt = (dim + kSymTile - 1) / kSymTile;
+  tile_items.release();
+  tile_part.release();
   // Rows are padded to a multiple of 16 complex entries (128 B in FP32):
   // every row starts 128-byte aligned, and the tensor-core GEMM reads the
   // matrix through a TMA map whose row pitch must be a multiple of 16 bytes.
@@ -611,13 +650,34 @@ lum_status CachedOperator::apply(const double2* x, double2* y, cudaStream_t st,
   if (packed) {
     const unsigned tiles = (unsigned)((size_t)nt * (nt + 1) / 2);
     if (precision == LUM_FP32)
-      gemv_sym_tiles<float2><<<tiles, kSymWarps * 32, 0, st>>>(
-          dim, nt, A.as<float2>(), sym_items.as<int2>(), x, sym_part.as<double2>(), skip);
+      gemv_sym_tiles<float2, false><<<tiles, kSymWarps * 32, 0, st>>>(
+          dim, nt, ld, A.as<float2>(), tile_items.as<int2>(), x, tile_part.as<double2>(), skip);
     else
-      gemv_sym_tiles<double2><<<tiles, kSymWarps * 32, 0, st>>>(
-          dim, nt, A.as<double2>(), sym_items.as<int2>(), x, sym_part.as<double2>(), skip);
+      gemv_sym_tiles<double2, false><<<tiles, kSymWarps * 32, 0, st>>>(
+          dim, nt, ld, A.as<double2>(), tile_items.as<int2>(), x, tile_part.as<double2>(), skip);
     LUM_CHECK_LAUNCH();
-    gemv_reduce<<<(dim + 255) / 256, 256, 0, st>>>(dim, nt, sym_part.as<double2>(), y, skip);
+    gemv_reduce<<<(dim + 255) / 256, 256, 0, st>>>(dim, nt, tile_part.as<double2>(), y, skip);
+    LUM_CHECK_LAUNCH();
+    return LUM_OK;
+  }
+  // Dense rows: the block product (x_J held in registers per block, FP32
+  // arithmetic for FP32 storage) unless LUMINA_DENSE_GEMV=rows selects the
+  // row-chunk GEMV below.
+  static const bool rows_gemv = [] {
+    const char* e = std::getenv("LUMINA_DENSE_GEMV");
+    return e && std::string(e) == "rows";
+  }();
+  if (!rows_gemv) {
+    if (!tile_items.p) LUM_TRY(tile_blocks(false));
+    const unsigned blocks = (unsigned)((size_t)nt * nt);
+    if (precision == LUM_FP32)
+      gemv_sym_tiles<float2, true><<<blocks, kSymWarps * 32, 0, st>>>(
+          dim, nt, ld, A.as<float2>(), tile_items.as<int2>(), x, tile_part.as<double2>(), skip);
+    else
+      gemv_sym_tiles<double2, true><<<blocks, kSymWarps * 32, 0, st>>>(
+          dim, nt, ld, A.as<double2>(), tile_items.as<int2>(), x, tile_part.as<double2>(), skip);
+    LUM_CHECK_LAUNCH();
+    gemv_reduce<<<(dim + 255) / 256, 256, 0, st>>>(dim, nt, tile_part.as<double2>(), y, skip);
     LUM_CHECK_LAUNCH();
     return LUM_OK;
   }

@@ -253,10 +253,11 @@ struct CachedOperator {
   // Symmetric tile storage (A = A^T): A holds the upper-triangle tiles,
   // packed row by row, each tile row-major with zero padding past dim.
   bool packed = false;
-  int nt = 0;               // tiles per side, ceil(dim / kSymTile)
-  DevBuf sym_items;         // int2 (I, J) per stored tile
-  DevBuf sym_part;          // double2 [nt][dim]: slot S, row r (see cached.cu)
+  int nt = 0;               // tiles (blocks) per side, ceil(dim / kSymTile)
+  DevBuf tile_items;        // int2 (I, J) per tile product block
+  DevBuf tile_part;         // double2 [nt][dim]: slot S, row r (see cached.cu)
   lum_status allocate(int dim, int precision, bool packed = false);
+  lum_status tile_blocks(bool upper);
   lum_status upload(const double* host, cudaStream_t st);
   lum_status assemble(const OtfOperator& geo, cudaStream_t st);
   lum_status apply(const double2* x, double2* y, cudaStream_t st, const int* skip = nullptr);
