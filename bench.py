@@ -603,8 +603,8 @@ def main():
     return 0
 
 
-def _traffic_from_profiles(kernel="otf_pairs_f32"):
-    path = os.path.join(ROOT, "profiles", f"{kernel}_cuboid30k.md")
+def _traffic_from_profiles(kernel="otf_pairs_f32", workload="cuboid30k"):
+    path = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.md")
     try:
         with open(path) as f:
             for line in f:
@@ -932,9 +932,13 @@ def _bench_cached(args, bk, stream, torch, lb, configs):
                          "kernel": ("gemv_part<float2> + gemv_reduce"
                                     if os.environ.get("LUMINA_DENSE_GEMV") == "rows" else
                                     "gemv_sym_tiles<float2, dense rows> + gemv_reduce"),
+                         # DRAM bytes of one launch from the ncu capture of this workload
+                         "traffic_source": "profiles/gemv_dense_blocks_cuboid6k.md",
                          "achieved": a_bytes / (ms_gemv * 1e-3) / 1e9, "peak": hbm_peak,
                          "unit": "GB/s", "frac": a_bytes / (ms_gemv * 1e-3) / 1e9 / hbm_peak,
-                         "traffic": None, "peak_source": hbm_src},
+                         "traffic": (_traffic_from_profiles("gemv_dense_blocks", "cuboid6k")
+                                     if os.environ.get("LUMINA_DENSE_GEMV") != "rows" else None),
+                         "peak_source": hbm_src},
             "tensor_product": {
                 "kernel": "cgemm_tf32x3_kernel", "nrhs": R, "ms": ms_tc,
                 "complex_tflops": cflops / (ms_tc * 1e-3) / 1e12,
