@@ -1514,6 +1514,30 @@ def _bench_metasurface(args, bk, stream, torch, lb, configs):
                          "applications": applies, "traffic": None},
             "per_wavelength": rows,
             "e2e": None}
+    if not args.no_e2e:
+        # e2e: the same wavelengths through CdaSolver with host arrays (its
+        # on-the-fly branch with the lattice sum and the Fresnel image; a new
+        # session per wavelength, as k_bloch changes with it), setup included
+        t_e2e = 0.0
+        for lam in lams:
+            pw = configs.metasurface(spacing=spacing, wavelength_nm=lam)
+            w = pw.workload
+            solver = lb.CdaSolver(backend=bk, iterative_threshold=0, use_fcd=True,
+                                  cell_size=w.cell_size, lattice=pw.lattice,
+                                  incident_field=pw.incident, matrix_memory_budget=0,
+                                  precision="fp32_refine", use_fft=False)
+            params = lb.SimulationParams(solver_tolerance=tol, max_iterations=max_iter,
+                                         k_bloch=pw.k_bloch, substrate_runtime=pw.substrate)
+            ds = lb.DipoleSet(w.positions, w.alpha)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            solver.compute_cross_sections(ds, lam, params)
+            t_e2e += time.perf_counter() - t0
+            solver.close()
+        line["e2e"] = {"value": n * len(lams) / t_e2e, "unit": UNIT,
+                       "h2d_bytes_per_step": n * (24 + 144),
+                       "d2h_bytes_per_step": n * 48,
+                       "includes": "session setup (lattice tables) per wavelength"}
     if not args.no_cpu:
         t_mv, nrows, dt, nt = cpu_matvec_sample(w0, args.cpu_seconds, periodic=pw0)
         line["cpu_baseline"] = {
