@@ -36,6 +36,19 @@ def test_ctypes_table_covers_header():
     assert _declared() == set(_ffi.SIGNATURES)
 
 
+def test_constants_match_header():
+    """Every LUM_* enumerator of the header that the ctypes mirror defines
+    has the header's value (status codes, precisions, solve modes, the
+    symmetric storage flag)."""
+    text = "".join(open(h).read() for h in glob.glob(os.path.join(ROOT, "include", "*.h")))
+    values = {n: int(v, 0) for n, v in re.findall(r"\b(LUM_[A-Z0-9_]+)\s*=\s*(0x[0-9a-fA-F]+|\d+)",
+                                                   text)}
+    checked = [n for n in values if hasattr(_ffi, n)]
+    assert "LUM_STORAGE_SYMMETRIC" in checked and "LUM_ERR_TIMEOUT" in checked
+    for n in checked:
+        assert getattr(_ffi, n) == values[n], n
+
+
 def test_no_device_means_unavailable():
     import torch
     if torch.cuda.is_available():
