@@ -78,3 +78,31 @@ def test_host_helpers_without_device():
     assert np.allclose(cs, ref, rtol=1e-12, atol=0)
     with pytest.raises(lb.InvalidGeometry):
         lb.invert_polarisability(np.zeros((1, 3, 3)))
+
+
+def test_cdasolver_storage_choice_without_device():
+    """CdaSolver's dispatch (cda/mod.rs:271-391) keeps the reference's branch
+    choice and picks symmetric tiles only for free-space cached systems."""
+    import numpy as np
+
+    import lumina_b200 as lb
+    from lumina_b200.lattice import LatticeSpec, SubstrateRuntime
+    pos = np.stack(np.meshgrid(*[np.arange(6.0)] * 3, indexing="ij"), -1).reshape(-1, 3) * 2.0
+    pos = pos + 0.1 * np.sin(np.arange(pos.size)).reshape(pos.shape)  # off the lattice: no FFT
+    ds = lb.DipoleSet(pos, np.tile(np.eye(3, dtype=complex), (pos.shape[0], 1, 1)))
+    free = lb.SimulationParams()
+    sub = lb.SimulationParams(substrate_runtime=SubstrateRuntime(-5.0, complex(0.2)))
+
+    def plan(params, direct=False, **kw):
+        s = lb.CdaSolver(backend=object(), cell_size=2.0, **kw)
+        branch, storage, _ = s._plan(ds, params, direct)
+        return branch, storage
+
+    assert plan(free, direct=True) == ("cached", "fp64+sym")
+    assert plan(free) == ("cached", "fp64+sym")
+    assert plan(free, precision="fp32_refine") == ("cached", "fp32+sym")
+    assert plan(free, symmetric_storage=False) == ("cached", "fp64")
+    assert plan(sub) == ("cached", "fp64")
+    lat = LatticeSpec.planar((400.0, 0.0, 0.0), (0.0, 400.0, 0.0))
+    assert plan(free, lattice=lat) == ("cached", "fp64")
+    assert plan(free, matrix_memory_budget=0) == ("onthefly", None)
