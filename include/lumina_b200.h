@@ -154,7 +154,8 @@ LUM_API int lum_session_upload_matrix(lum_session* s, const double* A);
  * assemble_interaction_matrix (assembly.rs:45-175): the whole 3N x 3N matrix
  * is built on the device.  inv_alpha = compute_diagonal_blocks output.
  * storage_precision | LUM_STORAGE_SYMMETRIC stores the upper-triangle tiles
- * only; INVALID with a lattice or a substrate (there A is not symmetric).
+ * only; INVALID with a lattice sum (which is not symmetric) or a substrate
+ * (the tile assembly covers free space only).
  * Such a session applies its matrix one vector per product: a tensor-core
  * product, or a lum_session_matmul_device of more than one vector, returns
  * INVALID, and lum_session_matmul_vectors and the right-hand-side batches
